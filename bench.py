@@ -1,0 +1,447 @@
+"""Assembly throughput benchmark (assembled CSR nonzeros per second).
+
+One step = one pass of the system-assembly hot path over the workload:
+element matrices (curl-curl, mass and k-parallel terms with the PML
+stretch), dual face transform, DOF signs, essential elimination and the
+atomic-free gather into the CSR values, all on device-resident inputs
+(``lfasm_assemble``).
+
+Default workload: the line grating (pitch 64 nm, CD 32 nm, 60 nm absorber
+over a 40 nm underlayer, 64 x 16 nm cell, lambda 13.5 nm, theta 6 deg,
+Nedelec p = 3, ~1.35M complex DOF), the configuration of the reference's
+published GPU assembly timing.  Synthetic, seeded mesh (no external data).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path does not shard a single mesh; N ranks run independent
+replicas (weak scaling), value = total nonzeros / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "assembly nnz/s"
+UNIT = "nnz/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(case, a) -> dict:
+    return {"workload": case.name + f" (~{case.ad.height / 1e6:.2f}M DOF)",
+            "p": case.p, "theta_deg": case.theta, "elements": case.ad.ne,
+            "ndof": case.ad.height, "nnz": int(case.nnz) if hasattr(case, "nnz") else None,
+            "l2_policy": "inputs larger than L2 (element buffer and CSR >> 126 MB)",
+            "replicas": a.gpus, "scale": a.scale}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def fp64_peak_tflops(torch) -> float:
+    """Measured FP64 reference peak: cuBLAS DGEMM 8192^3, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def cpu_baseline_reference(case, budget_s: float, threads: int) -> dict:
+    """The reference's serial CPU reassembler (reassemble_all,
+    solver/asm_data.inc:374-402, compiled from its sources) on a bounded
+    element sample; with threads > 1 each thread runs it on its own sample."""
+    from oracle import oracle
+    ne = case.ad.ne
+    kind = "reference" if oracle.ref_available() else "port"
+    rng = np.random.default_rng(7)
+    # calibrate on a small sample
+    probe = np.sort(rng.choice(ne, size=min(ne, 200), replace=False))
+    t_probe = _time_sample(case, probe, kind)
+    per_el = max(t_probe / len(probe), 1e-7)
+    m = int(min(ne, max(50, budget_s / per_el / max(threads, 1))))
+    samples = [np.sort(rng.choice(ne, size=m, replace=False)) for _ in range(threads)]
+    import concurrent.futures as cf
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda s: _time_sample(case, s, kind), samples))
+    wall = time.perf_counter() - t0
+    elems = m * threads
+    value = case.nnz * (elems / ne) / wall
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{elems} of {ne} elements ({threads} thread(s) x {m}), reassemble_all "
+                      f"on the sample's own CSR; nnz/s = full nnz x sampled fraction / wall",
+            "seconds": wall}
+
+
+def _time_sample(case, elements, kind) -> float:
+    from oracle import oracle
+    if kind == "reference":
+        rc = oracle.RefContext(case.ad, case.prob, elements=elements)
+        rc.build_csr()
+        return rc.time_reassemble()
+    import copy
+    sub = _subset_ad(case.ad, elements)
+    I, J = oracle.csr(sub)
+    t0 = time.perf_counter()
+    oracle.assemble(sub, case.prob, I, J, sub.ess, eliminate=False)
+    return time.perf_counter() - t0
+
+
+def _subset_ad(ad, elements):
+    import copy
+    sub = copy.copy(ad)
+    nd = ad.nd
+    sub.ne = len(elements)
+    sub.dof = np.ascontiguousarray(ad.dof.reshape(ad.ne, nd)[elements].reshape(-1))
+    sub.sign = np.ascontiguousarray(ad.sign.reshape(ad.ne, nd)[elements].reshape(-1))
+    sub.fo = np.ascontiguousarray(ad.fo.reshape(ad.ne, 4)[elements].reshape(-1)) if ad.p > 1 else ad.fo
+    sub.attr = np.ascontiguousarray(ad.attr[elements])
+    for k, w in (("J", 9), ("Jinv", 9), ("detJ", 1), ("v0", 3)):
+        setattr(sub, k, np.ascontiguousarray(getattr(ad, k).reshape(ad.ne, w)[elements].reshape(-1)))
+    sub.ess = np.zeros(0, dtype=np.int32)
+    return sub
+
+
+def dist_setup(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_setup(a)
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if a.impl == "reference":
+        return run_reference(a, rank, world, dist)
+    return run_ours(a, rank, world, local, dist, torch)
+
+
+def run_reference(a, rank, world, dist):
+    from lithofem_b200 import configs
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    case = configs.config(a.config, scale=a.scale)
+    case.nnz = _nnz_of(case)
+    threads = os.cpu_count() or 1
+    budget = 4.0
+    vals = []
+    info = None
+    for it in range(a.warmup + a.steps):
+        info = cpu_baseline_reference(case, budget, threads)
+        if it >= a.warmup:
+            vals.append(info["value"])
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * case.nnz / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(case, a),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _nnz_of(case) -> int:
+    """nnz of the symbolic CSR, from a device build when a GPU is present."""
+    from lithofem_b200.space import csr_symbolic
+    if case.ad.Jcol is not None:
+        return int(case.ad.Jcol.shape[0])
+    try:
+        import torch
+        if torch.cuda.is_available():
+            from lithofem_b200.asm import AsmGpuGlobal
+            g = AsmGpuGlobal(case.prob)
+            if g.Init(case.ad, 0) and g.BuildGlobal(case.ad.ess):
+                n = g.nnz()
+                g.Release()
+                return n
+    except Exception:
+        pass
+    I, J = csr_symbolic(case.ad)
+    return int(J.shape[0])
+
+
+def run_ours(a, rank, world, local, dist, torch):
+    from lithofem_b200 import _lib, configs
+    from lithofem_b200.asm import AsmGpuGlobal
+    dev = local
+    torch.cuda.set_device(dev)
+    case = configs.config(a.config, scale=a.scale)
+    ad, prob = case.ad, case.prob
+    stream = torch.cuda.current_stream()
+    g = AsmGpuGlobal(prob)
+    assert g.Init(ad, dev), "lfasm_init failed"
+    assert g.SetStream(stream.cuda_stream)
+    assert g.BuildGlobal(ad.ess)
+    case.nnz = g.nnz()
+    nb, npml = g.PathCounts()
+    # warm-up
+    for _ in range(a.warmup):
+        assert g.Assemble(True)
+    # per-stage profile (separate, untimed pass)
+    assert g.SetProfile(True)
+    stages = np.zeros(3)
+    nprof = 3
+    for _ in range(nprof):
+        assert g.Assemble(True)
+        stages += np.array(g.StageTimes())
+    stages /= nprof
+    assert g.SetProfile(False)
+    torch.cuda.synchronize()
+
+    # timed region: K steps on resident inputs, device events on the stream
+    assert g.SetAsync(True)
+    clk = ClockSampler(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    launches0 = _lib.lib().lfasm_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        if not g.Assemble(True):
+            raise RuntimeError("assembly failed")
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    launches = _lib.lib().lfasm_launch_count() - launches0
+    clocks = clk.stop()
+    assert g.SetAsync(False)
+    ms = ev0.elapsed_time(ev1) / a.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = case.nnz * world / (ms * 1e-3)
+
+    # e2e through the C ABI with host buffers: init (uploads from pinned host
+    # memory) + build_global + assemble + download of the CSR values
+    e2e = run_e2e(a, case, dev, torch, stream)
+
+    if rank != 0:
+        g.Release()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # roofline for the dominant stage
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    hbm_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    nd = ad.nd
+    alg = {
+        "bulk": nb * (nd * nd * 16 + 320 + 8 * 3),
+        "gather": ad.ne * nd * nd * (16 + 2) + ad.ne * nd * 4 + (ad.height + 1) * 8
+                  + case.nnz * 16,
+    }
+    rm, rc = ad.rule_mass, ad.rule_cc
+    rows = 3 * rc.nq + (6 if prob.has_kpar else 3) * rm.nq
+    pml_flops = npml * 4.0 * rows * nd * nd
+    fp64 = fp64_peak_tflops(torch)
+    stage_names = ["prep+bulk", "pml", "gather"]
+    kern = {}
+    for nm, t in zip(stage_names, stages):
+        kern[nm] = {"ms": float(t), "share": float(t / stages.sum())}
+    kern["prep+bulk"]["GB/s"] = alg["bulk"] / (stages[0] * 1e-3) / 1e9
+    kern["gather"]["GB/s"] = alg["gather"] / (stages[2] * 1e-3) / 1e9
+    kern["pml"]["TFLOP/s"] = pml_flops / (stages[1] * 1e-3) / 1e12 if stages[1] > 0 else 0.0
+    top = int(np.argmax(stages))
+    if top == 1:
+        ach = kern["pml"]["TFLOP/s"]
+        roof = {"kernel": "k_pml (PML elements, FP64 quadrature contraction)", "bound": "fp64",
+                "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
+                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3", "traffic": None}
+    else:
+        nm = stage_names[top]
+        ach = kern[nm]["GB/s"]
+        roof = {"kernel": {"prep+bulk": "k_bulk", "gather": "k_gather"}[nm], "bound": "hbm",
+                "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
+    prof_path = ROOT / "profiles" / "traffic.json"
+    if prof_path.exists():
+        try:
+            tr = json.loads(prof_path.read_text())
+            roof["traffic"] = tr.get(roof["kernel"].split()[0])
+        except Exception:
+            pass
+
+    cpu = None
+    if not a.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_baseline_reference(case, a.cpu_seconds, 1)
+            cpu.pop("seconds", None)
+        except Exception as exc:  # report, never fake
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"failed: {exc}"}
+
+    cfg = workload_config(case, a)
+    cfg["nnz"] = int(case.nnz)
+    cfg["bulk_elements"], cfg["pml_elements"] = nb, npml
+    cfg["parallelism"] = f"replicas x{world}"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
+            "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64}
+    print(json.dumps(line), flush=True)
+    g.Release()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_e2e(a, case, dev, torch, stream) -> dict:
+    from lithofem_b200.asm import AsmGpuGlobal
+    import copy
+    ad = copy.copy(case.ad)
+    h2d = 0
+    # inputs in pinned host memory
+    for name in ("dof", "sign", "fo", "attr", "J", "Jinv", "detJ", "v0"):
+        arr = getattr(ad, name)
+        t = torch.empty(arr.shape, dtype=getattr(torch, str(arr.dtype)), pin_memory=True)
+        t.numpy()[...] = arr
+        setattr(ad, name, t.numpy())
+        h2d += arr.nbytes
+    for r in (ad.rule_cc, ad.rule_mass):
+        h2d += r.ip.nbytes + r.w.nbytes + r.vshape.nbytes + r.curl.nbytes
+    h2d += ad.ess.nbytes
+    nnz = case.nnz
+    out = torch.empty(2 * nnz, dtype=torch.float64, pin_memory=True)
+    from lithofem_b200.asm import DeviceVector
+    times = []
+    for it in range(1 + a.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = AsmGpuGlobal(case.prob)
+        assert g.Init(ad, dev)
+        assert g.BuildGlobal(ad.ess)
+        assert g.Assemble(True)
+        # D2H of the result (the CSR values) through a borrowed device view
+        _, _, V, _, nz = g._csr()
+        dv = torch.as_tensor(DeviceVector(V, (2 * nz,), "<f8"), device="cuda")
+        out.copy_(dv)
+        torch.cuda.synchronize()
+        del dv
+        g.Release()
+        t1 = time.perf_counter()
+        if it >= 1:
+            times.append(t1 - t0)
+    t = float(np.median(times))
+    return {"value": nnz / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(16 * nnz), "ms_per_step": 1e3 * t,
+            "what": "lfasm_init (uploads from pinned host arrays) + lfasm_build_global "
+                    "(device symbolic CSR + maps) + lfasm_assemble + D2H of the CSR values",
+            "timer": "host wall clock with device synchronize on both sides"}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * lfasm.h -- C ABI of the B200 (sm_100a) LithoFEM system-assembly library
+ * (liblfasm.so).
+ *
+ * Drop-in for the reference's in-process assembly classes
+ *   AsmGpu        solver/asm_gpu.inc:271-425
+ *   AsmGpuGlobal  solver/asm_gpu.inc:498-599
+ * fed by the same extracted per-mesh data (AsmData, solver/asm_data.inc:77-97)
+ * and problem tables (Problem/Region, solver/problem_common.inc:18-65).
+ *
+ * Conventions (all entry points):
+ *   - return 0 (LFASM_OK) on success, a nonzero LFASM_ERR_* code on failure;
+ *     lfasm_last_error() returns the message, and a CUDA failure also prints
+ *     one "asm_gpu: CUDA error '<msg>' at <file>:<line>" line, the reference's
+ *     diagnostic (asm_gpu.inc:255-263);
+ *   - plain pointers and sizes only; host arrays are read during the call;
+ *   - device buffers are owned by the handle and freed by lfasm_destroy; the
+ *     device CSR returned by lfasm_get_csr is borrowed (the cuDSS contract of
+ *     solver/cudss_solver.inc:75-110: int32 0-based row pointer, sorted int32
+ *     columns, interleaved complex128 {re, im} values, general matrix);
+ *   - work runs on the handle's stream (lfasm_set_stream, default: the legacy
+ *     default stream) and every stage ends with a stream synchronize, as the
+ *     reference's stages end with cudaDeviceSynchronize, unless the handle
+ *     was switched to asynchronous mode (lfasm_set_async).
+ *   - there is no CPU fallback: without a usable CUDA device every call that
+ *     needs one fails with LFASM_ERR_CUDA.
+ */
+#ifndef LFASM_H
+#define LFASM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  LFASM_OK = 0,
+  LFASM_ERR_ARG = 1,         /* invalid argument / inconsistent sizes      */
+  LFASM_ERR_CUDA = 2,        /* CUDA runtime error                         */
+  LFASM_ERR_UNSUPPORTED = 3, /* outside the supported envelope (p > 3 ...) */
+  LFASM_ERR_STATE = 4,       /* call order (e.g. scatter before build)     */
+  LFASM_ERR_CSR = 5          /* given sparsity misses an element coupling  */
+};
+
+/* Integrator selection bits, identical to the reference's mask enum
+ * (asm_gpu.inc:51-58). */
+enum {
+  LFASM_CURLCURL = 1, /* rule_cc:  curl-curl with Lambda^-1                 */
+  LFASM_MASS = 2,     /* rule_mass: -k0^2 eps Lambda mass                   */
+  LFASM_CROSS0 = 4,   /* rule_mass: MixedVectorCurl (i K Lambda^-1)         */
+  LFASM_CROSS1 = 8,   /* rule_mass: MixedVectorWeakCurl (i Lambda^-1 K)     */
+  LFASM_KLK = 16      /* rule_mass: -K Lambda^-1 K mass                     */
+};
+
+/* Region kinds (problem_common.inc:18-27, parse_problem_core :296-318). */
+enum {
+  LFASM_REGION_BACKGROUND = 0,
+  LFASM_REGION_FRUSTUM = 1,
+  LFASM_REGION_PML_BOTTOM = 2,
+  LFASM_REGION_PML_TOP = 3
+};
+
+/* Reference tables at one quadrature rule: AsmRefRule (asm_data.inc:38-45). */
+typedef struct lfasm_ref_rule {
+  int nq;
+  const double *ip;     /* nq*3 reference coordinates                      */
+  const double *w;      /* nq weights                                      */
+  const double *vshape; /* nq*nd*3, [q*nd*3 + k*3 + d]                      */
+  const double *curl;   /* nq*nd*3                                         */
+} lfasm_ref_rule;
+
+/* Per-mesh extracted data: AsmData (asm_data.inc:77-97). I/Jcol may be NULL:
+ * the symbolic CSR (build_csr_symbolic, asm_data.inc:178-210) is then built
+ * on the device by lfasm_build_global. */
+typedef struct lfasm_asm_data {
+  int ne, nd, p, height, has_kpar;
+  const int *dof;      /* ne*nd decoded global dof                         */
+  const double *sign;  /* ne*nd +-1                                        */
+  const int *fo;       /* ne*4 face orientations 0..5 (NULL for p = 1)     */
+  const int *attr;     /* ne 1-based region attribute                      */
+  const double *J;     /* ne*9 row-major Jacobian                          */
+  const double *Jinv;  /* ne*9 row-major inverse                           */
+  const double *detJ;  /* ne                                               */
+  const double *v0;    /* ne*3 image of the reference origin               */
+  lfasm_ref_rule rule_cc, rule_mass;
+  const int *I;        /* height+1 row pointer, or NULL                    */
+  const int *Jcol;     /* nnz sorted columns, or NULL                      */
+  long long nnz;
+} lfasm_asm_data;
+
+/* Problem scalars and region table the path reads (Problem,
+ * problem_common.inc:40-65; PML parameters, asm_gpu.inc:31-36). */
+typedef struct lfasm_problem {
+  double k0, kx, ky;
+  double z_min, z_max, pml_thick, pml_order, pml_target;
+  int n_regions;
+  const double *region_eps;       /* 2*n_regions {re, im}                  */
+  const int *region_kind;         /* n_regions LFASM_REGION_*              */
+  const int *region_slab;         /* n_regions                             */
+  const double *region_delta_eps; /* 2*n_regions, eps - eps_bg (frustum)   */
+  const double *elem_eps;         /* NULL, or 2*ne per-element eps that
+                                     overrides the region value            */
+} lfasm_problem;
+
+/* One incident-field part on every slab: SlabWave tables
+ * (problem_common.inc:11-16, filled at lithofem_solve.cpp:577-598).
+ * Arrays have n_slab entries; A/B are 3 complex {re, im} per slab. */
+typedef struct lfasm_incident_part {
+  int n_slab;
+  const double *qA, *qB; /* 2*n_slab                                       */
+  const double *zA, *zB; /* n_slab                                         */
+  const double *A, *B;   /* 6*n_slab                                       */
+} lfasm_incident_part;
+
+typedef struct lfasm_handle lfasm_handle;
+
+/* Last error message of the calling thread ("" if none). */
+const char *lfasm_last_error(void);
+
+/* Number of CUDA kernels this library launched in the process. */
+long long lfasm_launch_count(void);
+
+/* AsmGpu::Init (asm_gpu.inc:276-322): select device, upload geometry,
+ * topology, rules and coefficient tables, allocate the element-matrix
+ * buffer (ne*nd*nd complex128). */
+int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
+               lfasm_handle **out);
+
+/* Stream for all work of this handle (a cudaStream_t; NULL = default). */
+int lfasm_set_stream(lfasm_handle *h, void *stream);
+
+/* 0: every stage synchronizes its stream at the end (default);
+ * 1: stages return after enqueueing (errors surface at the next sync). */
+int lfasm_set_async(lfasm_handle *h, int async_mode);
+
+/* AsmGpu::ComputeLocal (asm_gpu.inc:326-351): element matrices of the
+ * integrators selected by mask_cc (rule_cc) and mask_mass (rule_mass), with
+ * the dual face-orientation transform when apply_te != 0 (p >= 2), into the
+ * handle's element buffer, row-major nd x nd per element, without dof signs. */
+int lfasm_compute_local(lfasm_handle *h, int mask_cc, int mask_mass, int apply_te);
+
+/* Device element buffer (borrowed): ne*nd*nd interleaved complex128. */
+int lfasm_get_local(lfasm_handle *h, void **d_local);
+
+/* AsmGpu::DownloadLocal (asm_gpu.inc:355-362), test-only: copies the element
+ * buffer (2*ne*nd*nd doubles) and prints the reference's test-download
+ * marker line "asm_gpu_test_download (test-only D2H)". */
+int lfasm_download_local(lfasm_handle *h, double *host_out);
+
+/* AsmGpuGlobal::BuildGlobal (asm_gpu.inc:501-514): upload the essential
+ * (PEC) dof list and build the device CSR: the given I/Jcol, or the symbolic
+ * CSR built on the device, plus the row -> (element, local row) map and the
+ * element-entry -> CSR-slot map used by the atomic-free scatter. */
+int lfasm_build_global(lfasm_handle *h, const int *ess_list, int n_ess);
+
+/* AsmGpuGlobal::ScatterEliminate (asm_gpu.inc:517-530): element buffer from
+ * lfasm_compute_local -> CSR values with dof signs; eliminate != 0 zeroes
+ * essential rows/columns and puts 1+0i on their diagonal. */
+int lfasm_scatter_eliminate(lfasm_handle *h, int eliminate);
+
+/* Production path, the fused equivalent of ComputeLocal(CURLCURL,
+ * MASS[|CROSS0|CROSS1|KLK when k-parallel != 0], te) + ScatterEliminate
+ * (lithofem_solve.cpp:782-788): element matrices are written with signs,
+ * transform and elimination applied, then gathered row-wise into the CSR. */
+int lfasm_assemble(lfasm_handle *h, int eliminate);
+
+/* AsmGpuGlobal accessors (asm_gpu.inc:579-583): borrowed device CSR. */
+int lfasm_get_csr(lfasm_handle *h, int **d_rowptr, int **d_cols, void **d_vals,
+                  int *n, long long *nnz);
+
+/* Host copy of the symbolic CSR (height+1 and nnz ints). */
+int lfasm_download_csr(lfasm_handle *h, int *host_I, int *host_J);
+
+/* AsmGpuGlobal::DownloadValues (asm_gpu.inc:569-577), test-only: 2*nnz
+ * doubles, prints the test-download marker line. */
+int lfasm_download_values(lfasm_handle *h, double *host_out);
+
+/* AsmGpuGlobal::Residual (asm_gpu.inc:533-565): ||A X - B|| / ||B|| with X
+ * and B host vectors in the production [re(0..n-1); im(0..n-1)] layout. */
+int lfasm_residual(lfasm_handle *h, const double *X, const double *B, double *rel);
+
+/* Device variant: x, b interleaved complex128 device vectors of length n. */
+int lfasm_residual_device(lfasm_handle *h, const void *d_x, const void *d_b,
+                          double *rel);
+
+/* y = A x on device vectors (interleaved complex128, length n). */
+int lfasm_spmv(lfasm_handle *h, const void *d_x, void *d_y);
+
+/* Scattered-field right-hand side (ScatterSource, problem_common.inc:218-266,
+ * assembled as the reference's ComplexLinearForm with
+ * VectorFEDomainLFIntegrator, lithofem_solve.cpp:678-684), using the
+ * rule_mass points.  Part i goes into column col_of_part[i] of d_b
+ * (n x ncol, column-major, interleaved complex128): parts sharing a column
+ * are summed (one source with s and p parts), distinct columns give a
+ * multi-RHS block.  Essential rows are zeroed (form_rhs_only,
+ * lithofem_solve.cpp:732-742) when eliminate != 0. */
+int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts,
+                       int n_parts, const int *col_of_part, int ncol,
+                       int eliminate, void *d_b);
+
+/* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
+ * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
+ * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the
+ * milliseconds of {coefficient prep + bulk elements, PML elements, CSR
+ * gather}. */
+int lfasm_set_profile(lfasm_handle *h, int on);
+int lfasm_stage_times(lfasm_handle *h, float *ms3);
+
+/* Element counts of the two device paths (elements whose quadrature points
+ * all lie outside the PML, and the rest). */
+int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml);
+
+void lfasm_destroy(lfasm_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LFASM_H */

@@ -1,0 +1,204 @@
+"""Host-side mirror of the reference's GPU assembly classes.
+
+``AsmGpu`` / ``AsmGpuGlobal`` keep the names, call order, argument meaning
+and error behaviour of solver/asm_gpu.inc:271-425 and :498-599: every stage
+returns ``True``/``False``, a CUDA failure prints the one-line
+``asm_gpu: CUDA error '<msg>' at <file>:<line>`` diagnostic, and the
+test-only downloads print the ``asm_gpu_test_download`` marker.  The
+problem tables the reference reads from its global ``prob`` are passed to
+the constructor.  Everything runs in liblfasm.so (CUDA, sm_100a); there is
+no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _lib
+from ._abi import CROSS0, CROSS1, CURLCURL, KLK, MASS, c_double_p, c_int_p, marshal, marshal_parts
+from .problem import Problem
+from .space import AsmData
+
+__all__ = ["AsmGpu", "AsmGpuGlobal", "CURLCURL", "MASS", "CROSS0", "CROSS1", "KLK",
+           "DeviceVector"]
+
+
+class DeviceVector:
+    """Minimal __cuda_array_interface__ view of a borrowed device buffer."""
+
+    def __init__(self, ptr: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 2,
+                                         "strides": None}
+
+
+class AsmGpu:
+    def __init__(self, prob: Problem):
+        self.prob = prob
+        self._h = ct.c_void_p()
+        self._ne = self._nd = 0
+        self._m = None
+
+    # -- helpers ---------------------------------------------------------
+    def _ok(self, rc: int) -> bool:
+        if rc != 0:
+            msg = _lib.lib().lfasm_last_error().decode(errors="replace")
+            if rc != 2:  # CUDA errors were already printed by the library
+                print(f"asm_gpu: {msg}", flush=True)
+            self.last_error = (rc, msg)
+            return False
+        return True
+
+    @property
+    def handle(self) -> ct.c_void_p:
+        return self._h
+
+    # -- AsmGpu (asm_gpu.inc:276-376) -------------------------------------
+    def Init(self, ad: AsmData, gpu_id: int = 0, with_csr: bool = False) -> bool:
+        L = _lib.lib()
+        self.Release()
+        self._m = marshal(ad, self.prob, with_csr=with_csr)
+        self._ne, self._nd = ad.ne, ad.nd
+        return self._ok(L.lfasm_init(ct.byref(self._m.ad), ct.byref(self._m.prob), gpu_id,
+                                     ct.byref(self._h)))
+
+    def SetStream(self, stream_ptr: int) -> bool:
+        return self._ok(_lib.lib().lfasm_set_stream(self._h, ct.c_void_p(stream_ptr)))
+
+    def SetAsync(self, on: bool) -> bool:
+        return self._ok(_lib.lib().lfasm_set_async(self._h, int(bool(on))))
+
+    def ComputeLocal(self, mask_cc: int, mask_mass: int, apply_te: bool) -> bool:
+        return self._ok(_lib.lib().lfasm_compute_local(self._h, mask_cc, mask_mass,
+                                                       int(bool(apply_te))))
+
+    def DownloadLocal(self) -> np.ndarray | None:
+        out = np.empty(2 * self._ne * self._nd * self._nd, dtype=np.float64)
+        if not self._ok(_lib.lib().lfasm_download_local(self._h, out.ctypes.data_as(c_double_p))):
+            return None
+        return out.view(np.complex128).reshape(self._ne, self._nd, self._nd)
+
+    def DeviceLocal(self) -> int:
+        p = ct.c_void_p()
+        _lib.check(_lib.lib().lfasm_get_local(self._h, ct.byref(p)))
+        return int(p.value or 0)
+
+    def SetProfile(self, on: bool) -> bool:
+        return self._ok(_lib.lib().lfasm_set_profile(self._h, int(bool(on))))
+
+    def StageTimes(self) -> list[float]:
+        """ms of {prep + bulk elements, PML elements, CSR gather} of the last Assemble."""
+        out = (ct.c_float * 3)()
+        _lib.check(_lib.lib().lfasm_stage_times(self._h, out))
+        return [float(x) for x in out]
+
+    def PathCounts(self) -> tuple[int, int]:
+        a, b = ct.c_int(), ct.c_int()
+        _lib.check(_lib.lib().lfasm_path_counts(self._h, ct.byref(a), ct.byref(b)))
+        return a.value, b.value
+
+    def ne(self) -> int:
+        return self._ne
+
+    def nd(self) -> int:
+        return self._nd
+
+    def Release(self) -> None:
+        if self._h:
+            _lib.lib().lfasm_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Release()
+        except Exception:  # interpreter shutdown
+            pass
+
+
+class AsmGpuGlobal(AsmGpu):
+    """Owns the device CSR handed zero-copy to the sparse solver."""
+
+    def BuildGlobal(self, ess_list) -> bool:
+        ess = np.ascontiguousarray(np.asarray(ess_list, dtype=np.int32))
+        self._ess = ess
+        return self._ok(_lib.lib().lfasm_build_global(
+            self._h, ess.ctypes.data_as(c_int_p) if ess.size else None, int(ess.size)))
+
+    def ScatterEliminate(self, eliminate: bool) -> bool:
+        return self._ok(_lib.lib().lfasm_scatter_eliminate(self._h, int(bool(eliminate))))
+
+    def Assemble(self, eliminate: bool = True) -> bool:
+        """Production path: fused ComputeLocal(CC, MASS[+kpar], te) + ScatterEliminate."""
+        return self._ok(_lib.lib().lfasm_assemble(self._h, int(bool(eliminate))))
+
+    def _csr(self):
+        I, J, V = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        n, nnz = ct.c_int(), ct.c_longlong()
+        _lib.check(_lib.lib().lfasm_get_csr(self._h, ct.byref(I), ct.byref(J), ct.byref(V),
+                                            ct.byref(n), ct.byref(nnz)))
+        return int(I.value or 0), int(J.value or 0), int(V.value or 0), n.value, nnz.value
+
+    def n(self) -> int:
+        return self._csr()[3]
+
+    def nnz(self) -> int:
+        return self._csr()[4]
+
+    def DeviceI(self) -> int:
+        return self._csr()[0]
+
+    def DeviceJ(self) -> int:
+        return self._csr()[1]
+
+    def DeviceValues(self) -> int:
+        return self._csr()[2]
+
+    def DeviceCsrViews(self):
+        """__cuda_array_interface__ views (I int32, J int32, vals complex128)."""
+        I, J, V, n, nnz = self._csr()
+        return (DeviceVector(I, (n + 1,), "<i4"), DeviceVector(J, (nnz,), "<i4"),
+                DeviceVector(V, (nnz,), "<c16"))
+
+    def DownloadCsr(self) -> tuple[np.ndarray, np.ndarray]:
+        _, _, _, n, nnz = self._csr()
+        I = np.empty(n + 1, dtype=np.int32)
+        J = np.empty(nnz, dtype=np.int32)
+        _lib.check(_lib.lib().lfasm_download_csr(self._h, I.ctypes.data_as(c_int_p),
+                                                 J.ctypes.data_as(c_int_p)))
+        return I, J
+
+    def DownloadValues(self) -> np.ndarray | None:
+        nnz = self.nnz()
+        out = np.empty(2 * nnz, dtype=np.float64)
+        if not self._ok(_lib.lib().lfasm_download_values(self._h, out.ctypes.data_as(c_double_p))):
+            return None
+        return out.view(np.complex128)
+
+    def Residual(self, X: np.ndarray, B: np.ndarray) -> tuple[bool, float]:
+        """||A X - B|| / ||B||; X, B in the production [re; im] 2n layout."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        rel = ct.c_double()
+        ok = self._ok(_lib.lib().lfasm_residual(self._h, X.ctypes.data_as(c_double_p),
+                                                B.ctypes.data_as(c_double_p), ct.byref(rel)))
+        return ok, rel.value
+
+    def ResidualDevice(self, x_ptr: int, b_ptr: int) -> tuple[bool, float]:
+        rel = ct.c_double()
+        ok = self._ok(_lib.lib().lfasm_residual_device(self._h, ct.c_void_p(x_ptr),
+                                                       ct.c_void_p(b_ptr), ct.byref(rel)))
+        return ok, rel.value
+
+    def SpMV(self, x_ptr: int, y_ptr: int) -> bool:
+        return self._ok(_lib.lib().lfasm_spmv(self._h, ct.c_void_p(x_ptr), ct.c_void_p(y_ptr)))
+
+    def AssembleRHS(self, parts, col_of_part, ncol: int, eliminate: bool, b_ptr: int) -> bool:
+        arr, keep = marshal_parts(parts)
+        cols = np.ascontiguousarray(np.asarray(col_of_part, dtype=np.int32))
+        ok = self._ok(_lib.lib().lfasm_assemble_rhs(
+            self._h, arr, len(parts), cols.ctypes.data_as(c_int_p), int(ncol),
+            int(bool(eliminate)), ct.c_void_p(b_ptr)))
+        del keep
+        return ok

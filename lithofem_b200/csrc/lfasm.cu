@@ -1,0 +1,884 @@
+// liblfasm: B200 (sm_100a) LithoFEM system assembly behind the C ABI of
+// include/lfasm.h.  Host side of the handle; the kernels live in
+// lfasm_kernels.cuh.
+//
+// Call sequence mirrors the reference (solver/lithofem_solve.cpp:765-795):
+//   lfasm_init          <- AsmGpu::Init            (asm_gpu.inc:276-322)
+//   lfasm_build_global  <- AsmGpuGlobal::BuildGlobal (asm_gpu.inc:501-514)
+//   lfasm_assemble      <- ComputeLocal + ScatterEliminate (asm_gpu.inc:326-351, 517-530)
+//   lfasm_get_csr       <- DeviceI/DeviceJ/DeviceValues  (asm_gpu.inc:579-583)
+//   lfasm_residual      <- Residual                (asm_gpu.inc:533-565)
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_scan.cuh>
+
+#include "../../include/lfasm.h"
+#include "lfasm_kernels.cuh"
+
+using namespace lfasm_dev;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define LF_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      std::printf("asm_gpu: CUDA error '%s' at %s:%d\n",                       \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+      std::fflush(stdout);                                                     \
+      return fail(LFASM_ERR_CUDA, "CUDA error '%s' at %s:%d",                  \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+    }                                                                          \
+  } while (0)
+
+#define LF_LAUNCHED() g_launches.fetch_add(1, std::memory_order_relaxed)
+
+template <typename T>
+cudaError_t upload(T *&dst, const T *src, size_t count) {
+  dst = nullptr;
+  if (count == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(&dst, count * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) { cudaFree((void *)p); p = nullptr; }
+}
+
+struct DevRule {
+  int nq = 0;
+  double *ip = nullptr, *w = nullptr, *v = nullptr, *c = nullptr;
+  Rule view() const { Rule r; r.nq = nq; r.ip = ip; r.w = w; r.v = v; r.c = c; return r; }
+};
+
+}  // namespace
+
+struct lfasm_handle {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int async_mode = 0;
+  int ne = 0, nd = 0, p = 0, n = 0, has_kpar = 0;
+  int ndp = 0, ndp4 = 0;
+  long long nnz = 0;
+  // element data
+  int *dof = nullptr;
+  double *sign = nullptr;
+  int *attr = nullptr;
+  double *J = nullptr, *Jinv = nullptr, *detJ = nullptr, *v0 = nullptr;
+  unsigned *fopack = nullptr;
+  unsigned long long *signmask = nullptr, *essmask = nullptr;
+  DevRule rcc, rm;
+  dcplx *eps_tab = nullptr, *elem_eps = nullptr;
+  PmlParams pml{};
+  int *bulk_list = nullptr, *pml_list = nullptr;
+  int n_bulk = 0, n_pml = 0;
+  double *S = nullptr;
+  double *rec = nullptr;
+  dcplx *Ae = nullptr;
+  // RHS data
+  int *slab_of = nullptr;
+  dcplx *delta = nullptr;
+  int *src_list = nullptr, *src_slot = nullptr;
+  int n_src = 0;
+  int max_src_slab = -1;  // largest slab index among RHS source elements
+  // global
+  int built = 0, locals_valid = 0;
+  int *I = nullptr, *Jc = nullptr;
+  dcplx *vals = nullptr;
+  unsigned char *ess = nullptr;
+  int *ea_ptr = nullptr, *ea = nullptr;
+  uint16_t *off = nullptr;
+  int max_row = 0;
+  double *partials = nullptr, *red = nullptr;
+  int n_part_blocks = 0;
+  // optional per-stage events of lfasm_assemble: prep+bulk, pml, gather
+  int profile = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // host copies of a caller-given symbolic CSR (read at init)
+  std::vector<int> h_I, h_J;
+};
+
+namespace {
+
+int sync_if(lfasm_handle *h) {
+  LF_CUDA(cudaGetLastError());
+  if (!h->async_mode) LF_CUDA(cudaStreamSynchronize(h->stream));
+  return LFASM_OK;
+}
+
+// Element-independent tables of the bulk path: S_t[k][l] = quadrature sums
+// of reference shape products with the element's own rules (exact for the
+// polynomial integrands), symmetric pairs folded (j <= j').
+void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
+  const int nd = ad->nd;
+  S.assign((size_t)NT_ALL * ndp * ndp, 0.0);
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  auto at = [&](int t, int k, int l) -> double & { return S[((size_t)t * ndp + k) * ndp + l]; };
+  const lfasm_ref_rule &rc = ad->rule_cc, &rm = ad->rule_mass;
+  for (int k = 0; k < nd; ++k)
+    for (int l = 0; l < nd; ++l) {
+      double rcc[9] = {0}, rvv[9] = {0}, rvc[9] = {0}, rcv[9] = {0};
+      for (int q = 0; q < rc.nq; ++q) {
+        const double *ck = rc.curl + ((size_t)q * nd + k) * 3;
+        const double *cl = rc.curl + ((size_t)q * nd + l) * 3;
+        const double w = rc.w[q];
+        for (int j = 0; j < 3; ++j)
+          for (int jj = 0; jj < 3; ++jj) rcc[j * 3 + jj] += w * ck[j] * cl[jj];
+      }
+      for (int q = 0; q < rm.nq; ++q) {
+        const double *vk = rm.vshape + ((size_t)q * nd + k) * 3;
+        const double *vl = rm.vshape + ((size_t)q * nd + l) * 3;
+        const double *ck = rm.curl + ((size_t)q * nd + k) * 3;
+        const double *cl = rm.curl + ((size_t)q * nd + l) * 3;
+        const double w = rm.w[q];
+        for (int j = 0; j < 3; ++j)
+          for (int jj = 0; jj < 3; ++jj) {
+            rvv[j * 3 + jj] += w * vk[j] * vl[jj];
+            rvc[j * 3 + jj] += w * vk[j] * cl[jj];
+            rcv[j * 3 + jj] += w * ck[j] * vl[jj];
+          }
+      }
+      for (int t = 0; t < 6; ++t) {
+        const int a = pa[t], b = pb[t];
+        at(t, k, l) = a == b ? rcc[a * 3 + a] : rcc[a * 3 + b] + rcc[b * 3 + a];
+        at(6 + t, k, l) = a == b ? rvv[a * 3 + a] : rvv[a * 3 + b] + rvv[b * 3 + a];
+      }
+      for (int t = 0; t < 9; ++t) {
+        at(12 + t, k, l) = rvc[t];
+        at(21 + t, k, l) = rcv[t];
+      }
+    }
+}
+
+// 2x2 blocks relating element-local face DOF pairs to the global pairs for
+// the six face permutations, derived from the tangent pairs
+// (b - a, c - a) vs (B - A, C - A); column-major like asm_data.inc:26-34.
+void build_tinv(double out[24]) {
+  const int perms[6][3] = {{0, 1, 2}, {1, 0, 2}, {1, 2, 0}, {2, 1, 0}, {2, 0, 1}, {0, 2, 1}};
+  const double G[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+  for (int o = 0; o < 6; ++o) {
+    const double *a = G[perms[o][0]], *b = G[perms[o][1]], *c = G[perms[o][2]];
+    const double m00 = b[0] - a[0], m01 = b[1] - a[1];
+    const double m10 = c[0] - a[0], m11 = c[1] - a[1];
+    out[4 * o + 0] = m00;
+    out[4 * o + 1] = m10;
+    out[4 * o + 2] = m01;
+    out[4 * o + 3] = m11;
+  }
+}
+
+inline double pml_s_host(const PmlParams &p, double z, double *im) {
+  double d = -1.0, smax = 0.0;
+  if (z < p.z_min) { d = (p.z_min - z) / p.thick; smax = p.smax_bot; }
+  else if (z > p.z_max) { d = (z - p.z_max) / p.thick; smax = p.smax_top; }
+  if (d < 0.0) { *im = 0.0; return 1.0; }
+  if (d > 1.0) d = 1.0;
+  *im = smax * std::pow(d, p.order);
+  return 1.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lfasm_last_error(void) { return g_err.c_str(); }
+
+long long lfasm_launch_count(void) { return g_launches.load(); }
+
+int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
+               lfasm_handle **out) {
+  g_err.clear();
+  if (!out) return fail(LFASM_ERR_ARG, "out handle pointer is NULL");
+  *out = nullptr;
+  if (!ad || !prob) return fail(LFASM_ERR_ARG, "NULL asm data or problem");
+  if (ad->ne <= 0) return fail(LFASM_ERR_ARG, "empty mesh (ne = %d)", ad->ne);
+  if (ad->p < 1 || ad->p > 3)
+    return fail(LFASM_ERR_UNSUPPORTED, "ND order p = %d outside the supported 1..3", ad->p);
+  const int nd = ad->p * (ad->p + 2) * (ad->p + 3) / 2;
+  if (ad->nd != nd) return fail(LFASM_ERR_ARG, "nd = %d does not match p = %d", ad->nd, ad->p);
+  if (ad->height <= 0) return fail(LFASM_ERR_ARG, "height must be positive");
+  if (!ad->dof || !ad->sign || !ad->attr || !ad->J || !ad->Jinv || !ad->detJ || !ad->v0)
+    return fail(LFASM_ERR_ARG, "missing element array");
+  if (ad->p >= 2 && !ad->fo) return fail(LFASM_ERR_ARG, "face orientations required for p >= 2");
+  if (ad->rule_cc.nq <= 0 || ad->rule_mass.nq <= 0 || !ad->rule_cc.ip || !ad->rule_mass.ip ||
+      !ad->rule_cc.curl || !ad->rule_mass.curl || !ad->rule_mass.vshape || !ad->rule_cc.w ||
+      !ad->rule_mass.w)
+    return fail(LFASM_ERR_ARG, "missing reference rule tables");
+  if (prob->n_regions <= 0 || !prob->region_eps || !prob->region_kind)
+    return fail(LFASM_ERR_ARG, "missing region table");
+  if (!(prob->pml_thick > 0.0) || !(prob->k0 > 0.0))
+    return fail(LFASM_ERR_ARG, "k0 and pml thickness must be positive");
+  const size_t ne = ad->ne;
+  const size_t nen = ne * nd;
+  for (size_t i = 0; i < nen; ++i)
+    if (ad->dof[i] < 0 || ad->dof[i] >= ad->height)
+      return fail(LFASM_ERR_ARG, "dof[%zu] = %d out of range [0, %d)", i, ad->dof[i], ad->height);
+  for (size_t e = 0; e < ne; ++e) {
+    if (ad->attr[e] < 1 || ad->attr[e] > prob->n_regions)
+      return fail(LFASM_ERR_ARG, "attr[%zu] = %d outside 1..%d", e, ad->attr[e], prob->n_regions);
+    if (!(ad->detJ[e] > 0.0))
+      return fail(LFASM_ERR_ARG, "detJ[%zu] not positive", e);
+  }
+  if (ad->p >= 2)
+    for (size_t i = 0; i < ne * 4; ++i)
+      if (ad->fo[i] < 0 || ad->fo[i] > 5)
+        return fail(LFASM_ERR_ARG, "fo[%zu] = %d outside 0..5", i, ad->fo[i]);
+
+  int ndev = 0;
+  LF_CUDA(cudaGetDeviceCount(&ndev));
+  if (gpu_id < 0 || gpu_id >= ndev)
+    return fail(LFASM_ERR_ARG, "gpu_id %d outside the %d visible devices", gpu_id, ndev);
+  LF_CUDA(cudaSetDevice(gpu_id));
+
+  lfasm_handle *h = new lfasm_handle();
+  h->dev = gpu_id;
+  h->ne = ad->ne;
+  h->nd = nd;
+  h->p = ad->p;
+  h->n = ad->height;
+  h->has_kpar = (prob->kx != 0.0 || prob->ky != 0.0) ? 1 : 0;
+  h->ndp = (nd + 1) & ~1;
+  h->ndp4 = (nd + 3) & ~3;
+  if (ad->I || ad->Jcol) {
+    if (!ad->I || !ad->Jcol || ad->nnz <= 0) {
+      delete h;
+      return fail(LFASM_ERR_ARG, "I and Jcol must be given together with nnz > 0");
+    }
+    if (ad->I[0] != 0 || ad->I[ad->height] != ad->nnz) {
+      delete h;
+      return fail(LFASM_ERR_ARG, "row pointer does not span [0, nnz)");
+    }
+    h->h_I.assign(ad->I, ad->I + ad->height + 1);
+    h->h_J.assign(ad->Jcol, ad->Jcol + ad->nnz);
+  }
+  auto bail = [&](int code) { lfasm_destroy(h); return code; };
+#define LF_CUDA_H(call)                                                        \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      std::printf("asm_gpu: CUDA error '%s' at %s:%d\n",                       \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+      std::fflush(stdout);                                                     \
+      fail(LFASM_ERR_CUDA, "CUDA error '%s' at %s:%d", cudaGetErrorString(e_), \
+           __FILE__, __LINE__);                                                \
+      return bail(LFASM_ERR_CUDA);                                             \
+    }                                                                          \
+  } while (0)
+
+  double tinv[24];
+  build_tinv(tinv);
+  LF_CUDA_H(cudaMemcpyToSymbol(c_tinv, tinv, sizeof(tinv)));
+
+  // packed per-element orientation and sign bits
+  std::vector<unsigned> fop(ne, 0u);
+  std::vector<unsigned long long> sm(ne, 0ull);
+  for (size_t e = 0; e < ne; ++e) {
+    if (ad->p >= 2)
+      for (int f = 0; f < 4; ++f) fop[e] |= (unsigned)ad->fo[e * 4 + f] << (8 * f);
+    for (int k = 0; k < nd; ++k)
+      if (ad->sign[e * nd + k] < 0.0) sm[e] |= 1ull << k;
+  }
+  LF_CUDA_H(upload(h->dof, ad->dof, nen));
+  LF_CUDA_H(upload(h->sign, ad->sign, nen));
+  LF_CUDA_H(upload(h->attr, ad->attr, ne));
+  LF_CUDA_H(upload(h->J, ad->J, ne * 9));
+  LF_CUDA_H(upload(h->Jinv, ad->Jinv, ne * 9));
+  LF_CUDA_H(upload(h->detJ, ad->detJ, ne));
+  LF_CUDA_H(upload(h->v0, ad->v0, ne * 3));
+  LF_CUDA_H(upload(h->fopack, fop.data(), ne));
+  LF_CUDA_H(upload(h->signmask, sm.data(), ne));
+  auto up_rule = [&](DevRule &d, const lfasm_ref_rule &r) -> cudaError_t {
+    d.nq = r.nq;
+    cudaError_t e;
+    if ((e = upload(d.ip, r.ip, (size_t)r.nq * 3)) != cudaSuccess) return e;
+    if ((e = upload(d.w, r.w, (size_t)r.nq)) != cudaSuccess) return e;
+    if (r.vshape && (e = upload(d.v, r.vshape, (size_t)r.nq * nd * 3)) != cudaSuccess) return e;
+    return upload(d.c, r.curl, (size_t)r.nq * nd * 3);
+  };
+  LF_CUDA_H(up_rule(h->rcc, ad->rule_cc));
+  LF_CUDA_H(up_rule(h->rm, ad->rule_mass));
+
+  std::vector<dcplx> eps(prob->n_regions);
+  for (int r = 0; r < prob->n_regions; ++r)
+    eps[r] = dcplx{prob->region_eps[2 * r], prob->region_eps[2 * r + 1]};
+  LF_CUDA_H(upload(h->eps_tab, eps.data(), eps.size()));
+  if (prob->elem_eps) {
+    LF_CUDA_H(upload(h->elem_eps, reinterpret_cast<const dcplx *>(prob->elem_eps), ne));
+  }
+
+  PmlParams &pm = h->pml;
+  pm.z_min = prob->z_min;
+  pm.z_max = prob->z_max;
+  pm.thick = prob->pml_thick;
+  pm.order = prob->pml_order;
+  pm.k0 = prob->k0;
+  pm.kx = prob->kx;
+  pm.ky = prob->ky;
+  double n_bot = 1.0, n_top = 1.0;
+  for (int r = 0; r < prob->n_regions; ++r) {
+    const double er = prob->region_eps[2 * r], ei = prob->region_eps[2 * r + 1];
+    // |sqrt(eps)| = |eps|^(1/2)
+    const double nm = std::sqrt(std::sqrt(er * er + ei * ei));
+    if (prob->region_kind[r] == LFASM_REGION_PML_BOTTOM) n_bot = nm;
+    if (prob->region_kind[r] == LFASM_REGION_PML_TOP) n_top = nm;
+  }
+  pm.smax_bot = -std::log(prob->pml_target) * (prob->pml_order + 1) /
+                (2.0 * prob->k0 * n_bot * prob->pml_thick);
+  pm.smax_top = -std::log(prob->pml_target) * (prob->pml_order + 1) /
+                (2.0 * prob->k0 * n_top * prob->pml_thick);
+
+  // classify: bulk iff s(z_q) == 1 exactly at every point of both rules
+  std::vector<int> bl, pl;
+  bl.reserve(ne);
+  for (size_t e = 0; e < ne; ++e) {
+    const double *J = ad->J + e * 9;
+    const double z0 = ad->v0[e * 3 + 2];
+    bool bulk = true;
+    for (int rr = 0; rr < 2 && bulk; ++rr) {
+      const lfasm_ref_rule &R = rr == 0 ? ad->rule_cc : ad->rule_mass;
+      for (int q = 0; q < R.nq && bulk; ++q) {
+        const double z = z0 + J[6] * R.ip[q * 3] + J[7] * R.ip[q * 3 + 1] + J[8] * R.ip[q * 3 + 2];
+        double im;
+        pml_s_host(pm, z, &im);
+        if (im != 0.0 || z < pm.z_min || z > pm.z_max) bulk = false;
+      }
+    }
+    (bulk ? bl : pl).push_back((int)e);
+  }
+  h->n_bulk = (int)bl.size();
+  h->n_pml = (int)pl.size();
+  LF_CUDA_H(upload(h->bulk_list, bl.data(), bl.size()));
+  LF_CUDA_H(upload(h->pml_list, pl.data(), pl.size()));
+  if (h->n_bulk) LF_CUDA_H(cudaMalloc(&h->rec, (size_t)h->n_bulk * REC * sizeof(double)));
+
+  std::vector<double> S;
+  build_S(ad, h->ndp, S);
+  LF_CUDA_H(upload(h->S, S.data(), S.size()));
+
+  // RHS source elements: frustum regions (delta = region eps - eps_bg) or,
+  // with per-element eps, every non-PML element whose eps differs from its
+  // slab background.
+  {
+    std::vector<int> slab(ne, 0), src, slot(ne, -1);
+    std::vector<dcplx> del(ne, dcplx{0.0, 0.0});
+    std::vector<int> bg_of_slab(prob->n_regions + 1, -1);
+    int max_slab = 0;
+    for (int r = 0; r < prob->n_regions; ++r)
+      if (prob->region_slab) max_slab = std::max(max_slab, prob->region_slab[r]);
+    std::vector<int> bg(max_slab + 2, -1);
+    for (int r = 0; r < prob->n_regions; ++r)
+      if (prob->region_kind[r] == LFASM_REGION_BACKGROUND && prob->region_slab &&
+          prob->region_slab[r] >= 0)
+        bg[prob->region_slab[r]] = r;
+    for (size_t e = 0; e < ne; ++e) {
+      const int r = ad->attr[e] - 1;
+      const int kind = prob->region_kind[r];
+      slab[e] = prob->region_slab ? prob->region_slab[r] : 0;
+      dcplx d{0.0, 0.0};
+      if (kind == LFASM_REGION_FRUSTUM && prob->region_delta_eps)
+        d = dcplx{prob->region_delta_eps[2 * r], prob->region_delta_eps[2 * r + 1]};
+      if (prob->elem_eps && (kind == LFASM_REGION_BACKGROUND || kind == LFASM_REGION_FRUSTUM) &&
+          slab[e] >= 0 && bg[slab[e]] >= 0) {
+        const int b = bg[slab[e]];
+        d = dcplx{prob->elem_eps[2 * e] - prob->region_eps[2 * b],
+                  prob->elem_eps[2 * e + 1] - prob->region_eps[2 * b + 1]};
+      }
+      del[e] = d;
+      if (d.re != 0.0 || d.im != 0.0) {
+        slot[e] = (int)src.size();
+        src.push_back((int)e);
+        h->max_src_slab = std::max(h->max_src_slab, slab[e]);
+      }
+    }
+    h->n_src = (int)src.size();
+    LF_CUDA_H(upload(h->slab_of, slab.data(), ne));
+    LF_CUDA_H(upload(h->delta, del.data(), ne));
+    LF_CUDA_H(upload(h->src_list, src.data(), src.size()));
+    LF_CUDA_H(upload(h->src_slot, slot.data(), ne));
+  }
+
+  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * nd * sizeof(dcplx)));
+  LF_CUDA_H(cudaDeviceSynchronize());
+#undef LF_CUDA_H
+  *out = h;
+  return LFASM_OK;
+}
+
+int lfasm_set_stream(lfasm_handle *h, void *stream) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  h->stream = (cudaStream_t)stream;
+  return LFASM_OK;
+}
+
+int lfasm_set_async(lfasm_handle *h, int async_mode) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  h->async_mode = async_mode ? 1 : 0;
+  return LFASM_OK;
+}
+
+int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (n_bulk) *n_bulk = h->n_bulk;
+  if (n_pml) *n_pml = h->n_pml;
+  return LFASM_OK;
+}
+
+static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int mode,
+                        int eliminate) {
+  if ((mask_cc & ~LFASM_CURLCURL) || (mask_mass & LFASM_CURLCURL) || (mask_mass & ~31))
+    return fail(LFASM_ERR_UNSUPPORTED,
+                "mask_cc may select only CURLCURL and mask_mass only MASS|CROSS0|CROSS1|KLK");
+  LF_CUDA(cudaSetDevice(h->dev));
+  const int mask = mask_cc | mask_mass;
+  const bool cross = (mask & (LFASM_CROSS0 | LFASM_CROSS1)) != 0;
+  const bool prof = mode == 1 && h->profile;
+  // every element is written by exactly one of the two paths: no memset
+  if (prof) LF_CUDA(cudaEventRecord(h->ev[0], h->stream));
+  if (h->n_bulk) {
+    const int nb = h->n_bulk;
+    k_prep_bulk<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
+                                                         h->detJ, h->attr, h->eps_tab,
+                                                         h->elem_eps, h->pml, mask, h->rec);
+    LF_LAUNCHED();
+    const int chunk = 16;
+    const int ytiles = ((h->ndp / 2) * h->ndp + BULK_THREADS - 1) / BULK_THREADS;
+    dim3 grid((nb + chunk - 1) / chunk, ytiles);
+#define LF_BULK(C, M)                                                             \
+  k_bulk<C, M><<<grid, BULK_THREADS, 0, h->stream>>>(                             \
+      nb, h->bulk_list, h->rec, h->S, h->nd, h->ndp, h->p, chunk, te, eliminate,  \
+      h->fopack, h->signmask, h->essmask, h->Ae)
+    if (cross) { if (mode) LF_BULK(true, 1); else LF_BULK(true, 0); }
+    else { if (mode) LF_BULK(false, 1); else LF_BULK(false, 0); }
+#undef LF_BULK
+    LF_LAUNCHED();
+  }
+  if (prof) LF_CUDA(cudaEventRecord(h->ev[1], h->stream));
+  if (h->n_pml) {
+    const int tpr = h->ndp4 / 4;
+    const int threads = ((tpr * tpr + 31) / 32) * 32;
+    const size_t smem = (size_t)PML_QC * 6 * h->ndp4 * (sizeof(double) + sizeof(dcplx)) +
+                        PML_QC * sizeof(QCoef);
+#define LF_PML(C, M)                                                                 \
+  do {                                                                               \
+    LF_CUDA(cudaFuncSetAttribute(k_pml<C, M>,                                        \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                                 (int)smem));                                        \
+    k_pml<C, M><<<h->n_pml, threads, smem, h->stream>>>(                             \
+        h->n_pml, h->pml_list, h->nd, h->ndp4, h->p, h->rcc.view(), h->rm.view(),    \
+        h->J, h->Jinv, h->detJ, h->v0, h->attr, h->eps_tab, h->elem_eps, h->pml,     \
+        mask_cc, mask_mass, te, eliminate, h->fopack, h->signmask, h->essmask,       \
+        h->Ae);                                                                      \
+  } while (0)
+    if (cross) { if (mode) LF_PML(true, 1); else LF_PML(true, 0); }
+    else { if (mode) LF_PML(false, 1); else LF_PML(false, 0); }
+#undef LF_PML
+    LF_LAUNCHED();
+  }
+  if (prof) LF_CUDA(cudaEventRecord(h->ev[2], h->stream));
+  return LFASM_OK;
+}
+
+int lfasm_compute_local(lfasm_handle *h, int mask_cc, int mask_mass, int apply_te) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  g_err.clear();
+  if (!mask_cc && !mask_mass) {
+    LF_CUDA(cudaSetDevice(h->dev));
+    LF_CUDA(cudaMemsetAsync(h->Ae, 0, (size_t)h->ne * h->nd * h->nd * sizeof(dcplx), h->stream));
+  } else {
+    int rc = launch_local(h, mask_cc, mask_mass, apply_te ? 1 : 0, 0, 0);
+    if (rc) return rc;
+  }
+  h->locals_valid = 1;
+  return sync_if(h);
+}
+
+int lfasm_get_local(lfasm_handle *h, void **d_local) {
+  if (!h || !d_local) return fail(LFASM_ERR_ARG, "NULL argument");
+  *d_local = h->Ae;
+  return LFASM_OK;
+}
+
+int lfasm_download_local(lfasm_handle *h, double *host_out) {
+  if (!h || !host_out) return fail(LFASM_ERR_ARG, "NULL argument");
+  std::printf("asm_gpu_test_download (test-only D2H)\n");
+  std::fflush(stdout);
+  LF_CUDA(cudaSetDevice(h->dev));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  LF_CUDA(cudaMemcpy(host_out, h->Ae, (size_t)h->ne * h->nd * h->nd * sizeof(dcplx),
+                     cudaMemcpyDeviceToHost));
+  return LFASM_OK;
+}
+
+}  // extern "C"
+
+// symbolic CSR + row maps
+static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long nnz_given) {
+  const int n = h->n, nd = h->nd;
+  const long long total = (long long)h->ne * nd;
+  int *cnt = nullptr, *fill = nullptr, *dmax = nullptr, *err = nullptr;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0;
+  LF_CUDA(cudaMalloc(&cnt, (size_t)(n + 1) * sizeof(int)));
+  LF_CUDA(cudaMalloc(&fill, (size_t)n * sizeof(int)));
+  LF_CUDA(cudaMalloc(&dmax, 2 * sizeof(int)));
+  LF_CUDA(cudaMalloc(&err, sizeof(int)));
+  LF_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(n + 1) * sizeof(int), h->stream));
+  LF_CUDA(cudaMemsetAsync(fill, 0, (size_t)n * sizeof(int), h->stream));
+  LF_CUDA(cudaMemsetAsync(dmax, 0, 2 * sizeof(int), h->stream));
+  LF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), h->stream));
+  LF_CUDA(cudaMalloc(&h->ea_ptr, (size_t)(n + 1) * sizeof(int)));
+  LF_CUDA(cudaMalloc(&h->ea, (size_t)total * sizeof(int)));
+  const int tb = 256;
+  const unsigned gb = (unsigned)((total + tb - 1) / tb);
+  k_count_rows<<<gb, tb, 0, h->stream>>>(total, h->dof, cnt);
+  LF_LAUNCHED();
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, h->ea_ptr, n + 1, h->stream));
+  LF_CUDA(cudaMalloc(&tmp, tmp_bytes));
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, h->ea_ptr, n + 1, h->stream));
+  k_fill_rows<<<gb, tb, 0, h->stream>>>(total, h->dof, h->ea_ptr, fill, h->ea);
+  LF_LAUNCHED();
+  k_max_reduce<<<256, 256, 0, h->stream>>>(n, h->ea_ptr, 1, dmax);
+  LF_LAUNCHED();
+  int mmax = 0;
+  LF_CUDA(cudaMemcpyAsync(&mmax, dmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  if (mmax > 64) {
+    cudaFree(cnt); cudaFree(fill); cudaFree(dmax); cudaFree(err); cudaFree(tmp);
+    return fail(LFASM_ERR_UNSUPPORTED, "a dof belongs to %d elements (max 64)", mmax);
+  }
+  int cap = 32;
+  while (cap < mmax * nd) cap <<= 1;
+  const int wpb = 4;
+  const size_t smem = (size_t)wpb * (cap + 64) * sizeof(int);
+  const unsigned rb = (unsigned)((n + wpb - 1) / wpb);
+  LF_CUDA(cudaMalloc(&h->off, (size_t)total * nd * sizeof(uint16_t)));
+  if (!hI) {
+    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_row_symbolic<1><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
+                                                          cnt, nullptr, nullptr, nullptr, err);
+    LF_LAUNCHED();
+    LF_CUDA(cudaMalloc(&h->I, (size_t)(n + 1) * sizeof(int)));
+    LF_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int), h->stream));
+    LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, h->I, n + 1, h->stream));
+    int nnz = 0;
+    LF_CUDA(cudaMemcpyAsync(&nnz, h->I + n, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    LF_CUDA(cudaStreamSynchronize(h->stream));
+    h->nnz = nnz;
+    LF_CUDA(cudaMalloc(&h->Jc, (size_t)std::max(nnz, 1) * sizeof(int)));
+    k_row_symbolic<2><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
+                                                          nullptr, h->I, h->Jc, h->off, err);
+    LF_LAUNCHED();
+  } else {
+    // sort each row's list (pass 1 without counting) then map into the
+    // caller's sparsity
+    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_row_symbolic<1><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
+                                                          cnt, nullptr, nullptr, nullptr, err);
+    LF_LAUNCHED();
+    h->nnz = nnz_given;
+    LF_CUDA(upload(h->I, hI, (size_t)n + 1));
+    LF_CUDA(upload(h->Jc, hJ, (size_t)nnz_given));
+    const size_t smem3 = (size_t)wpb * (cap + 64) * sizeof(int);
+    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+    k_row_symbolic<3><<<rb, wpb * 32, smem3, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
+                                                           nullptr, h->I, h->Jc, h->off, err);
+    LF_LAUNCHED();
+  }
+  k_max_reduce<<<256, 256, 0, h->stream>>>(n, h->I, 1, dmax + 1);
+  LF_LAUNCHED();
+  int herr = 0, mrow = 0;
+  LF_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaMemcpyAsync(&mrow, dmax + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  cudaFree(cnt); cudaFree(fill); cudaFree(dmax); cudaFree(err); cudaFree(tmp);
+  if (herr == 1) return fail(LFASM_ERR_CSR, "CSR position missing: the given sparsity lacks an element coupling");
+  if (herr) return fail(LFASM_ERR_UNSUPPORTED, "row map overflow");
+  if (mrow > 65535) return fail(LFASM_ERR_UNSUPPORTED, "row with %d entries exceeds 65535", mrow);
+  h->max_row = std::max(mrow, 1);
+  return LFASM_OK;
+}
+
+static int build_global_csr(lfasm_handle *h, const int *hI, const int *hJ, long long nnz) {
+  int rc = build_maps(h, hI, hJ, nnz);
+  if (rc) return rc;
+  LF_CUDA(cudaMalloc(&h->vals, (size_t)std::max<long long>(h->nnz, 1) * sizeof(dcplx)));
+  h->n_part_blocks = (h->n + 7) / 8;
+  LF_CUDA(cudaMalloc(&h->partials, (size_t)h->n_part_blocks * 2 * sizeof(double)));
+  LF_CUDA(cudaMalloc(&h->red, 2 * sizeof(double)));
+  h->built = 1;
+  return sync_if(h);
+}
+
+extern "C" {
+
+int lfasm_build_global(lfasm_handle *h, const int *ess_list, int n_ess) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  g_err.clear();
+  if (h->built) return fail(LFASM_ERR_STATE, "global structure already built");
+  if (n_ess < 0 || (n_ess > 0 && !ess_list)) return fail(LFASM_ERR_ARG, "bad essential list");
+  LF_CUDA(cudaSetDevice(h->dev));
+  std::vector<unsigned char> ess(h->n, 0);
+  for (int i = 0; i < n_ess; ++i) {
+    if (ess_list[i] < 0 || ess_list[i] >= h->n)
+      return fail(LFASM_ERR_ARG, "essential dof %d out of range", ess_list[i]);
+    ess[ess_list[i]] = 1;
+  }
+  LF_CUDA(upload(h->ess, ess.data(), ess.size()));
+  LF_CUDA(cudaMalloc(&h->essmask, (size_t)h->ne * sizeof(unsigned long long)));
+  k_essmask<<<(h->ne + 255) / 256, 256, 0, h->stream>>>(h->ne, h->nd, h->dof, h->ess, h->essmask);
+  LF_LAUNCHED();
+  if (h->h_I.empty()) return build_global_csr(h, nullptr, nullptr, 0);
+  return build_global_csr(h, h->h_I.data(), h->h_J.data(), (long long)h->h_J.size());
+}
+
+static int gather(lfasm_handle *h, bool raw, int eliminate) {
+  const int wpb = 8;
+  const size_t smem = (size_t)wpb * h->max_row * sizeof(dcplx);
+  const unsigned nb = (unsigned)((h->n + wpb - 1) / wpb);
+  if (raw) {
+    LF_CUDA(cudaFuncSetAttribute(k_gather<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gather<true><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
+                                                      h->Ae, h->nd, h->ess, h->sign, h->dof,
+                                                      eliminate, h->max_row, h->vals);
+  } else {
+    LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gather<false><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
+                                                       h->Ae, h->nd, h->ess, h->sign, h->dof,
+                                                       eliminate, h->max_row, h->vals);
+  }
+  LF_LAUNCHED();
+  return LFASM_OK;
+}
+
+int lfasm_scatter_eliminate(lfasm_handle *h, int eliminate) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  g_err.clear();
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  if (!h->locals_valid) return fail(LFASM_ERR_STATE, "lfasm_compute_local has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  int rc = gather(h, true, eliminate ? 1 : 0);
+  if (rc) return rc;
+  return sync_if(h);
+}
+
+int lfasm_assemble(lfasm_handle *h, int eliminate) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  g_err.clear();
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
+  int rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, eliminate ? 1 : 0);
+  if (rc) return rc;
+  h->locals_valid = 0;  // the element buffer now holds signed entries
+  rc = gather(h, false, eliminate ? 1 : 0);
+  if (rc) return rc;
+  if (h->profile) LF_CUDA(cudaEventRecord(h->ev[3], h->stream));
+  return sync_if(h);
+}
+
+int lfasm_set_profile(lfasm_handle *h, int on) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  LF_CUDA(cudaSetDevice(h->dev));
+  if (on && !h->ev[0])
+    for (int i = 0; i < 4; ++i) LF_CUDA(cudaEventCreate(&h->ev[i]));
+  h->profile = on ? 1 : 0;
+  return LFASM_OK;
+}
+
+int lfasm_stage_times(lfasm_handle *h, float *ms3) {
+  if (!h || !ms3) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->profile) return fail(LFASM_ERR_STATE, "profiling is off");
+  LF_CUDA(cudaSetDevice(h->dev));
+  LF_CUDA(cudaEventSynchronize(h->ev[3]));
+  for (int i = 0; i < 3; ++i) LF_CUDA(cudaEventElapsedTime(ms3 + i, h->ev[i], h->ev[i + 1]));
+  return LFASM_OK;
+}
+
+int lfasm_get_csr(lfasm_handle *h, int **d_rowptr, int **d_cols, void **d_vals, int *n,
+                  long long *nnz) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  if (d_rowptr) *d_rowptr = h->I;
+  if (d_cols) *d_cols = h->Jc;
+  if (d_vals) *d_vals = h->vals;
+  if (n) *n = h->n;
+  if (nnz) *nnz = h->nnz;
+  return LFASM_OK;
+}
+
+int lfasm_download_csr(lfasm_handle *h, int *host_I, int *host_J) {
+  if (!h || !host_I || !host_J) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  LF_CUDA(cudaMemcpy(host_I, h->I, (size_t)(h->n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  LF_CUDA(cudaMemcpy(host_J, h->Jc, (size_t)h->nnz * sizeof(int), cudaMemcpyDeviceToHost));
+  return LFASM_OK;
+}
+
+int lfasm_download_values(lfasm_handle *h, double *host_out) {
+  if (!h || !host_out) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  std::printf("asm_gpu_test_download (test-only D2H)\n");
+  std::fflush(stdout);
+  LF_CUDA(cudaSetDevice(h->dev));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  LF_CUDA(cudaMemcpy(host_out, h->vals, (size_t)h->nnz * sizeof(dcplx), cudaMemcpyDeviceToHost));
+  return LFASM_OK;
+}
+
+static int residual_core(lfasm_handle *h, const dcplx *dx, const dcplx *db, double *rel) {
+  const int wpb = 8;
+  const unsigned nb = (unsigned)((h->n + wpb - 1) / wpb);
+  k_spmv_resid<<<nb, wpb * 32, 0, h->stream>>>(h->n, h->I, h->Jc, h->vals, dx, db, nullptr,
+                                                h->partials);
+  LF_LAUNCHED();
+  k_sum_partials<<<1, 1024, 0, h->stream>>>((int)nb, h->partials, h->red);
+  LF_LAUNCHED();
+  double hr[2];
+  LF_CUDA(cudaMemcpyAsync(hr, h->red, sizeof(hr), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  *rel = hr[1] > 0.0 ? std::sqrt(hr[0] / hr[1]) : 0.0;
+  return LFASM_OK;
+}
+
+int lfasm_residual(lfasm_handle *h, const double *X, const double *B, double *rel) {
+  if (!h || !X || !B || !rel) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  double *d2 = nullptr;
+  dcplx *dx = nullptr, *db = nullptr;
+  const size_t n = h->n;
+  LF_CUDA(cudaMalloc(&d2, 2 * n * sizeof(double)));
+  LF_CUDA(cudaMalloc(&dx, n * sizeof(dcplx)));
+  LF_CUDA(cudaMalloc(&db, n * sizeof(dcplx)));
+  const unsigned g = (unsigned)((n + 255) / 256);
+  LF_CUDA(cudaMemcpyAsync(d2, X, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_split_to_cplx<<<g, 256, 0, h->stream>>>((int)n, d2, dx);
+  LF_LAUNCHED();
+  LF_CUDA(cudaMemcpyAsync(d2, B, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_split_to_cplx<<<g, 256, 0, h->stream>>>((int)n, d2, db);
+  LF_LAUNCHED();
+  int rc = residual_core(h, dx, db, rel);
+  cudaFree(d2);
+  cudaFree(dx);
+  cudaFree(db);
+  return rc;
+}
+
+int lfasm_residual_device(lfasm_handle *h, const void *d_x, const void *d_b, double *rel) {
+  if (!h || !d_x || !d_b || !rel) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  return residual_core(h, (const dcplx *)d_x, (const dcplx *)d_b, rel);
+}
+
+int lfasm_spmv(lfasm_handle *h, const void *d_x, void *d_y) {
+  if (!h || !d_x || !d_y) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  const int wpb = 8;
+  const unsigned nb = (unsigned)((h->n + wpb - 1) / wpb);
+  k_spmv_resid<<<nb, wpb * 32, 0, h->stream>>>(h->n, h->I, h->Jc, h->vals, (const dcplx *)d_x,
+                                                nullptr, (dcplx *)d_y, nullptr);
+  LF_LAUNCHED();
+  return sync_if(h);
+}
+
+int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts, int n_parts,
+                       const int *col_of_part, int ncol, int eliminate, void *d_b) {
+  if (!h || (n_parts > 0 && (!parts || !col_of_part)) || ncol <= 0 || !d_b)
+    return fail(LFASM_ERR_ARG, "bad RHS arguments");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  int n_slab = n_parts > 0 ? parts[0].n_slab : 1;
+  if (n_parts > 0 && h->max_src_slab >= n_slab)
+    return fail(LFASM_ERR_ARG, "incident tables have %d slabs; source elements reach slab %d",
+                n_slab, h->max_src_slab);
+  std::vector<SlabWaveD> waves((size_t)std::max(n_parts, 1) * n_slab);
+  for (int pi = 0; pi < n_parts; ++pi) {
+    const lfasm_incident_part &P = parts[pi];
+    if (P.n_slab != n_slab) return fail(LFASM_ERR_ARG, "parts disagree on the slab count");
+    if (col_of_part[pi] < 0 || col_of_part[pi] >= ncol)
+      return fail(LFASM_ERR_ARG, "part %d mapped to column %d of %d", pi, col_of_part[pi], ncol);
+    for (int s = 0; s < n_slab; ++s) {
+      SlabWaveD &w = waves[(size_t)pi * n_slab + s];
+      w.qA = dcplx{P.qA[2 * s], P.qA[2 * s + 1]};
+      w.qB = dcplx{P.qB[2 * s], P.qB[2 * s + 1]};
+      w.zA = P.zA[s];
+      w.zB = P.zB[s];
+      for (int d = 0; d < 3; ++d) {
+        w.A[d] = dcplx{P.A[6 * s + 2 * d], P.A[6 * s + 2 * d + 1]};
+        w.B[d] = dcplx{P.B[6 * s + 2 * d], P.B[6 * s + 2 * d + 1]};
+      }
+    }
+  }
+  SlabWaveD *dw = nullptr;
+  int *dcol = nullptr;
+  dcplx *be = nullptr;
+  LF_CUDA(upload(dw, waves.data(), waves.size()));
+  std::vector<int> cols(col_of_part, col_of_part + n_parts);
+  if (n_parts) LF_CUDA(upload(dcol, cols.data(), cols.size()));
+  if (h->n_src) LF_CUDA(cudaMalloc(&be, (size_t)h->n_src * ncol * h->nd * sizeof(dcplx)));
+  if (h->n_src && n_parts) {
+    const int wpb = 4;
+    k_rhs_elem<<<(h->n_src + wpb - 1) / wpb, wpb * 32, 0, h->stream>>>(
+        h->n_src, h->src_list, h->nd, h->p, h->rm.view(), h->J, h->Jinv, h->detJ, h->v0,
+        h->slab_of, h->delta, dw, n_slab, n_parts, dcol, ncol, h->pml.k0, h->fopack, be);
+    LF_LAUNCHED();
+  } else if (h->n_src) {
+    LF_CUDA(cudaMemsetAsync(be, 0, (size_t)h->n_src * ncol * h->nd * sizeof(dcplx), h->stream));
+  }
+  k_rhs_gather<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->n, h->ea_ptr, h->ea, h->nd,
+                                                          h->src_slot, h->sign, be, ncol, h->ess,
+                                                          eliminate ? 1 : 0, (dcplx *)d_b);
+  LF_LAUNCHED();
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  cudaFree(dw);
+  if (dcol) cudaFree(dcol);
+  if (be) cudaFree(be);
+  return sync_if(h);
+}
+
+void lfasm_destroy(lfasm_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->dev);
+  dfree(h->dof); dfree(h->sign); dfree(h->attr); dfree(h->J); dfree(h->Jinv); dfree(h->detJ);
+  dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
+  for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
+  dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
+  dfree(h->S); dfree(h->rec); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
+  dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
+  dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->off); dfree(h->partials);
+  dfree(h->red);
+  for (int i = 0; i < 4; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  delete h;
+}
+
+}  // extern "C"

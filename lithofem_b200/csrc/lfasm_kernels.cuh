@@ -1,0 +1,829 @@
+// Device kernels of liblfasm (sm_100a).  Included once by lfasm.cu.
+//
+// Element-matrix evaluation follows the reference's arithmetic
+// (solver/asm_gpu.inc:70-214 and the CPU twin solver/asm_data.inc:218-370):
+// physical shapes v = refv . Jinv, curls c = J . refc / detJ, weight
+// w_q detJ, PML stretch s(z) per quadrature point (asm_gpu.inc:40-48) and the
+// five integrator tensors.  Two device paths share that arithmetic:
+//
+//  * bulk elements (every quadrature point outside the PML, where s == 1
+//    exactly): the integrand coefficients are constant on the element, so
+//    A_e = sum_t G_e[t] S_t with 3x3 geometry coefficients G_e (from J, Jinv,
+//    detJ, eps, k-parallel) and element-independent tables S_t of reference
+//    quadrature sums (w_q refX_k,j refY_l,j'), evaluated with the same rules
+//    and exact for these polynomial integrands;
+//  * PML elements: per-quadrature-point contraction A += X_q^T (W_q X_q)
+//    with X_q the (face-transformed) physical shapes and W_q the complex
+//    coefficient tensors, register-tiled over 4x4 entry blocks.
+
+#pragma once
+
+#include <cstdint>
+
+namespace lfasm_dev {
+
+struct dcplx {
+  double re, im;
+};
+
+struct PmlParams {  // asm_gpu.inc:31-36
+  double z_min, z_max, thick, order;
+  double smax_bot, smax_top;
+  double k0, kx, ky;
+};
+
+struct Rule {
+  int nq;
+  const double *ip, *w, *v, *c;
+};
+
+constexpr int REC = 40;        // doubles per bulk-element coefficient record
+constexpr int NT_CC = 6;       // symmetric (j <= j') pairs
+constexpr int NT_ALL = 30;     // 6 cc + 6 vv + 9 vc + 9 cv
+constexpr int BULK_THREADS = 128;
+constexpr int MAXND = 48;
+
+__constant__ double c_tinv[24];   // 2x2 column-major blocks per orientation
+
+__device__ __forceinline__ dcplx mk(double r, double i) { dcplx z; z.re = r; z.im = i; return z; }
+__device__ __forceinline__ dcplx cmul(dcplx a, dcplx b) {
+  return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__device__ __forceinline__ dcplx cinv(dcplx a) {
+  const double d = a.re * a.re + a.im * a.im;
+  return mk(a.re / d, -a.im / d);
+}
+__device__ __forceinline__ dcplx cscale(double s, dcplx a) { return mk(s * a.re, s * a.im); }
+__device__ __forceinline__ dcplx cadd(dcplx a, dcplx b) { return mk(a.re + b.re, a.im + b.im); }
+
+// PML stretch s(z) (problem_common.inc:69-90 with the per-side maximum
+// precomputed as at asm_gpu.inc:310-319).
+__device__ __forceinline__ dcplx pml_s(const PmlParams &p, double z) {
+  double d = -1.0, smax = 0.0;
+  if (z < p.z_min) { d = (p.z_min - z) / p.thick; smax = p.smax_bot; }
+  else if (z > p.z_max) { d = (z - p.z_max) / p.thick; smax = p.smax_top; }
+  if (d < 0.0) return mk(1.0, 0.0);
+  if (d > 1.0) d = 1.0;
+  return mk(1.0, smax * pow(d, p.order));
+}
+
+__device__ __forceinline__ int face_of(int k, int p) {
+  const int f0 = 6 * p, nf = p * (p - 1);
+  if (nf == 0 || k < f0 || k >= f0 + 4 * nf) return -1;
+  return (k - f0) / nf;
+}
+
+// ---------------------------------------------------------------------------
+// bulk-element coefficient records
+// rec layout: [0,6) gcc (real, pairs (00,11,22,01,02,12)), [6,18) gvv complex
+// pairs, [18,27) gvc (imaginary unit factored out, j*3+j'), [27,36) gcv.
+// ---------------------------------------------------------------------------
+__global__ void k_prep_bulk(int nb, const int *__restrict__ list,
+                            const double *__restrict__ J9, const double *__restrict__ Ji9,
+                            const double *__restrict__ detJ, const int *__restrict__ attr,
+                            const dcplx *__restrict__ eps_tab,
+                            const dcplx *__restrict__ elem_eps, PmlParams pml,
+                            int mask, double *__restrict__ rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const int e = list[i];
+  double J[9], Ji[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    J[t] = J9[(size_t)e * 9 + t];
+    Ji[t] = Ji9[(size_t)e * 9 + t];
+  }
+  const double det = detJ[e];
+  const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+  double *r = rec + (size_t)i * REC;
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  const bool cc = mask & 1, ms = mask & 2, c0 = mask & 4, c1 = mask & 8, kl = mask & 16;
+  const double kx = pml.kx, ky = pml.ky, k2 = pml.k0 * pml.k0;
+  // K = [[0,0,ky],[0,0,-kx],[-ky,kx,0]] (fill_K, problem_common.inc:150-158)
+  const double K[9] = {0.0, 0.0, ky, 0.0, 0.0, -kx, -ky, kx, 0.0};
+  // -K K (real symmetric), the bulk KLK tensor
+  const double mKK[9] = {ky * ky, -kx * ky, 0.0, -kx * ky, kx * kx, 0.0, 0.0, 0.0,
+                         kx * kx + ky * ky};
+  const double me_re = -k2 * eps.re, me_im = -k2 * eps.im;
+  for (int t = 0; t < 6; ++t) {
+    const int a = pa[t], b = pb[t];
+    double g = 0.0;
+    if (cc) g = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
+    r[t] = g;
+    // Jinv row a . Jinv row b
+    const double jj = Ji[a * 3 + 0] * Ji[b * 3 + 0] + Ji[a * 3 + 1] * Ji[b * 3 + 1] +
+                      Ji[a * 3 + 2] * Ji[b * 3 + 2];
+    double vr = 0.0, vi = 0.0;
+    if (ms) { vr += me_re * jj; vi += me_im * jj; }
+    if (kl) {
+      double s = 0.0;
+      for (int rr = 0; rr < 3; ++rr)
+        for (int cc2 = 0; cc2 < 3; ++cc2) s += Ji[a * 3 + rr] * mKK[rr * 3 + cc2] * Ji[b * 3 + cc2];
+      vr += s;
+    }
+    r[6 + 2 * t] = det * vr;
+    r[7 + 2 * t] = det * vi;
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double gvc = 0.0, gcv = 0.0;
+      for (int rr = 0; rr < 3; ++rr)
+        for (int cc2 = 0; cc2 < 3; ++cc2) {
+          const double k = K[rr * 3 + cc2];
+          if (k == 0.0) continue;
+          gvc += Ji[a * 3 + rr] * k * J[cc2 * 3 + b];
+          gcv += J[rr * 3 + a] * k * Ji[b * 3 + cc2];
+        }
+      r[18 + a * 3 + b] = c0 ? gvc : 0.0;
+      r[27 + a * 3 + b] = c1 ? gcv : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bulk element kernel: thread <-> (row pair I, column l); registers hold the
+// S-table values of its two entries; loops over a chunk of elements.
+// MODE 0: raw local matrix (ComputeLocal); MODE 1: signs + elimination.
+// ---------------------------------------------------------------------------
+template <bool CROSS, int MODE>
+__global__ void __launch_bounds__(BULK_THREADS)
+k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
+       const double *__restrict__ S, int nd, int ndp, int p, int chunk, int te,
+       int eliminate, const unsigned *__restrict__ fopack,
+       const unsigned long long *__restrict__ signmask,
+       const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
+  constexpr int NT = CROSS ? NT_ALL : 12;
+  const int f = blockIdx.y * BULK_THREADS + threadIdx.x;
+  const int half = ndp >> 1;
+  const int I = f / ndp, l = f - I * ndp;
+  const bool valid = I < half;
+  const int r0 = 2 * I, r1 = 2 * I + 1;
+  double s0[NT], s1[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    s0[t] = valid ? S[((size_t)t * ndp + r0) * ndp + l] : 0.0;
+    s1[t] = valid ? S[((size_t)t * ndp + r1) * ndp + l] : 0.0;
+  }
+  const int frow = valid ? face_of(r0, p) : -1;
+  const int fcol = valid ? face_of(l & ~1, p) : -1;
+  const int cp = l & 1;
+  const int i0 = blockIdx.x * chunk;
+  const int i1 = min(nb, i0 + chunk);
+  for (int i = i0; i < i1; ++i) {
+    const double *g = rec + (size_t)i * REC;
+    double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const double gc = __ldg(g + t);
+      re0 = fma(gc, s0[t], re0);
+      re1 = fma(gc, s1[t], re1);
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const double gr = __ldg(g + 6 + 2 * t), gi = __ldg(g + 7 + 2 * t);
+      re0 = fma(gr, s0[6 + t], re0);
+      im0 = fma(gi, s0[6 + t], im0);
+      re1 = fma(gr, s1[6 + t], re1);
+      im1 = fma(gi, s1[6 + t], im1);
+    }
+    if (CROSS) {
+#pragma unroll
+      for (int t = 0; t < 18; ++t) {
+        const double gi = __ldg(g + 18 + t);
+        im0 = fma(gi, s0[(12 + t) % NT], im0);
+        im1 = fma(gi, s1[(12 + t) % NT], im1);
+      }
+    }
+    const int e = __ldg(list + i);
+    if (te && p >= 2) {
+      const unsigned fp = __ldg(fopack + e);
+      // columns: A <- A M (partner column from the neighbouring lane)
+      const double pr0 = __shfl_xor_sync(0xffffffffu, re0, 1);
+      const double pi0 = __shfl_xor_sync(0xffffffffu, im0, 1);
+      const double pr1 = __shfl_xor_sync(0xffffffffu, re1, 1);
+      const double pi1 = __shfl_xor_sync(0xffffffffu, im1, 1);
+      if (fcol >= 0) {
+        const double *T = c_tinv + 4 * ((fp >> (8 * fcol)) & 0xffu);
+        // new[cp] = A[.][0] M[0][cp] + A[.][1] M[1][cp]; M[c'][c] = T[2c + c']
+        const double a0 = T[2 * cp + 0], a1 = T[2 * cp + 1];
+        const double own = cp == 0 ? a0 : a1, oth = cp == 0 ? a1 : a0;
+        const double nr0 = own * re0 + oth * pr0, ni0 = own * im0 + oth * pi0;
+        const double nr1 = own * re1 + oth * pr1, ni1 = own * im1 + oth * pi1;
+        re0 = nr0; im0 = ni0; re1 = nr1; im1 = ni1;
+      }
+      // rows: A <- M^T A
+      if (frow >= 0) {
+        const double *T = c_tinv + 4 * ((fp >> (8 * frow)) & 0xffu);
+        const double nr0 = T[0] * re0 + T[1] * re1, ni0 = T[0] * im0 + T[1] * im1;
+        const double nr1 = T[2] * re0 + T[3] * re1, ni1 = T[2] * im0 + T[3] * im1;
+        re0 = nr0; im0 = ni0; re1 = nr1; im1 = ni1;
+      }
+    }
+    if (MODE == 1 && valid) {
+      const unsigned long long sm = __ldg(signmask + e);
+      const double sl = ((sm >> l) & 1ull) ? -1.0 : 1.0;
+      const double sa = (((sm >> r0) & 1ull) ? -1.0 : 1.0) * sl;
+      const double sb = (((sm >> r1) & 1ull) ? -1.0 : 1.0) * sl;
+      re0 *= sa; im0 *= sa; re1 *= sb; im1 *= sb;
+      if (eliminate) {
+        const unsigned long long em = __ldg(essmask + e);
+        const bool el = (em >> l) & 1ull;
+        if (el || ((em >> r0) & 1ull)) { re0 = 0.0; im0 = 0.0; }
+        if (el || ((em >> r1) & 1ull)) { re1 = 0.0; im1 = 0.0; }
+      }
+    }
+    if (valid && l < nd) {
+      dcplx *dst = Ae + (size_t)e * nd * nd;
+      dst[(size_t)r0 * nd + l] = mk(re0, im0);
+      if (r1 < nd) dst[(size_t)r1 * nd + l] = mk(re1, im1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PML element kernel: one element per block, thread <-> 4x4 entry tile.
+// ---------------------------------------------------------------------------
+constexpr int PML_QC = 8;  // quadrature points staged per round
+
+struct QCoef {  // per quadrature point, already multiplied by w_q detJ
+  dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries
+  dcplx b02, b12, b20, b21;           // M0 = i K Lambda^-1
+  dcplx c02, c12, c20, c21;           // M1 = i Lambda^-1 K
+};
+
+template <bool CROSS, int MODE>
+__global__ void k_pml(int npml, const int *__restrict__ list, int nd, int ndp4, int p,
+                      Rule rcc, Rule rm, const double *__restrict__ J9,
+                      const double *__restrict__ Ji9, const double *__restrict__ detJ,
+                      const double *__restrict__ v0, const int *__restrict__ attr,
+                      const dcplx *__restrict__ eps_tab, const dcplx *__restrict__ elem_eps,
+                      PmlParams pml, int mask_cc, int mask_mass, int te, int eliminate,
+                      const unsigned *__restrict__ fopack,
+                      const unsigned long long *__restrict__ signmask,
+                      const unsigned long long *__restrict__ essmask,
+                      dcplx *__restrict__ Ae) {
+  extern __shared__ double smem[];
+  const int rows_q = CROSS ? 6 : 3;
+  const int maxrows = PML_QC * 6;
+  double *Xs = smem;                                    // maxrows * ndp4
+  dcplx *Ys = reinterpret_cast<dcplx *>(Xs + (size_t)maxrows * ndp4);  // maxrows*ndp4
+  QCoef *qc = reinterpret_cast<QCoef *>(Ys + (size_t)maxrows * ndp4); // PML_QC
+  __shared__ double sJ[9], sJi[9], sdet, sv0z;
+  __shared__ dcplx seps;
+  __shared__ unsigned sfo;
+
+  const int e = list[blockIdx.x];
+  const int tid = threadIdx.x;
+  if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
+  if (tid == 0) {
+    sdet = detJ[e];
+    sv0z = v0[(size_t)e * 3 + 2];
+    seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+    sfo = fopack[e];
+  }
+  __syncthreads();
+
+  const int tpr = ndp4 >> 2;               // tiles per row
+  const int ntile = tpr * tpr;
+  const bool active = tid < ntile;
+  const int ti = active ? tid / tpr : 0, tl = active ? tid - ti * tpr : 0;
+  double acc_re[4][4], acc_im[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { acc_re[a][b] = 0.0; acc_im[a][b] = 0.0; }
+
+  const double k2 = pml.k0 * pml.k0;
+  const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
+  const int npair = ndp4 >> 1;
+
+  for (int rule = 0; rule < 2; ++rule) {
+    const int mask = rule == 0 ? mask_cc : mask_mass;
+    if (!mask) continue;
+    const Rule R = rule == 0 ? rcc : rm;
+    const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+    const bool need_v = rule == 1;
+    const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+    (void)rows_q;
+    for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
+      const int nqc = min(PML_QC, R.nq - q0);
+      // per-point coefficients
+      if (tid < nqc) {
+        const int q = q0 + tid;
+        const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
+                         sJ[8] * R.ip[q * 3 + 2];
+        const dcplx s = pml_s(pml, z);
+        const dcplx si = cinv(s);
+        const double w = R.w[q] * sdet;
+        QCoef c;
+        if (rule == 0) {
+          // cc: a00 = w li0, a11 = w li1, a22 = w li2 (diagonal), rest unused
+          c.a00 = cscale(w, si); c.a11 = cscale(w, si); c.a22 = cscale(w, s);
+          c.a01 = mk(0, 0); c.a10 = mk(0, 0);
+          c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
+        } else {
+          const dcplx li0 = si, li1 = si, li2 = s;
+          dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
+          if (mask & 2) {
+            const dcplx me = cscale(-k2, seps);
+            a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
+          }
+          if (mask & 16) {
+            a00 = cadd(a00, cscale(-K02 * K20, li2));
+            a01 = cadd(a01, cscale(-K02 * K21, li2));
+            a10 = cadd(a10, cscale(-K12 * K20, li2));
+            a11 = cadd(a11, cscale(-K12 * K21, li2));
+            a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
+          }
+          c.a00 = cscale(w, a00); c.a01 = cscale(w, a01); c.a10 = cscale(w, a10);
+          c.a11 = cscale(w, a11); c.a22 = cscale(w, a22);
+          const dcplx iu = mk(0.0, 1.0);
+          if (mask & 4) {
+            c.b02 = cscale(w * K02, cmul(iu, li2)); c.b12 = cscale(w * K12, cmul(iu, li2));
+            c.b20 = cscale(w * K20, cmul(iu, li0)); c.b21 = cscale(w * K21, cmul(iu, li1));
+          } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
+          if (mask & 8) {
+            c.c02 = cscale(w * K02, cmul(iu, li0)); c.c12 = cscale(w * K12, cmul(iu, li1));
+            c.c20 = cscale(w * K20, cmul(iu, li2)); c.c21 = cscale(w * K21, cmul(iu, li2));
+          } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
+        }
+        qc[tid] = c;
+      }
+      __syncthreads();
+      // stage X (transformed physical shapes) and Y = W X, column pairs
+      for (int it = tid; it < nqc * npair; it += blockDim.x) {
+        const int qi = it / npair, pr = it - qi * npair;
+        const int q = q0 + qi;
+        double v[2][3], c[2][3];
+        for (int h = 0; h < 2; ++h) {
+          const int k = 2 * pr + h;
+          for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
+          if (k < nd) {
+            const double *rv = R.v + ((size_t)q * nd + k) * 3;
+            const double *rc = R.c + ((size_t)q * nd + k) * 3;
+            for (int d = 0; d < 3; ++d) {
+              if (need_v)
+                v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
+              if (need_c)
+                c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
+            }
+          }
+        }
+        if (te && p >= 2) {
+          const int f = face_of(2 * pr, p);
+          if (f >= 0) {
+            const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
+            for (int d = 0; d < 3; ++d) {
+              const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
+              v[0][d] = v0_ * T[0] + v1_ * T[1];
+              v[1][d] = v0_ * T[2] + v1_ * T[3];
+              c[0][d] = c0_ * T[0] + c1_ * T[1];
+              c[1][d] = c0_ * T[2] + c1_ * T[3];
+            }
+          }
+        }
+        const QCoef &C = qc[qi];
+        for (int h = 0; h < 2; ++h) {
+          const int k = 2 * pr + h;
+          const int rb = qi * rq;
+          if (rule == 0) {
+            for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + d) * ndp4 + k] = c[h][d];
+            Ys[(size_t)(rb + 0) * ndp4 + k] = cscale(c[h][0], C.a00);
+            Ys[(size_t)(rb + 1) * ndp4 + k] = cscale(c[h][1], C.a11);
+            Ys[(size_t)(rb + 2) * ndp4 + k] = cscale(c[h][2], C.a22);
+          } else {
+            for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + d) * ndp4 + k] = v[h][d];
+            const double *vv = v[h], *cc = c[h];
+            dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+            dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+            dcplx y2 = cscale(vv[2], C.a22);
+            if (need_c) {
+              y0 = cadd(y0, cscale(cc[2], C.b02));
+              y1 = cadd(y1, cscale(cc[2], C.b12));
+              y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+              for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + 3 + d) * ndp4 + k] = cc[d];
+              Ys[(size_t)(rb + 3) * ndp4 + k] = cscale(vv[2], C.c02);
+              Ys[(size_t)(rb + 4) * ndp4 + k] = cscale(vv[2], C.c12);
+              Ys[(size_t)(rb + 5) * ndp4 + k] = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+            }
+            Ys[(size_t)(rb + 0) * ndp4 + k] = y0;
+            Ys[(size_t)(rb + 1) * ndp4 + k] = y1;
+            Ys[(size_t)(rb + 2) * ndp4 + k] = y2;
+          }
+        }
+      }
+      __syncthreads();
+      if (active) {
+        const int nrows = nqc * rq;
+        for (int r = 0; r < nrows; ++r) {
+          const double *xr = Xs + (size_t)r * ndp4 + 4 * ti;
+          const dcplx *yr = Ys + (size_t)r * ndp4 + 4 * tl;
+          double x[4];
+          dcplx y[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) { x[a] = xr[a]; y[a] = yr[a]; }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+              acc_re[a][b] = fma(x[a], y[b].re, acc_re[a][b]);
+              acc_im[a][b] = fma(x[a], y[b].im, acc_im[a][b]);
+            }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (!active) return;
+  const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
+  const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+  dcplx *dst = Ae + (size_t)e * nd * nd;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int k = 4 * ti + a;
+    if (k >= nd) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int l = 4 * tl + b;
+      if (l >= nd) continue;
+      double re = acc_re[a][b], im = acc_im[a][b];
+      if (MODE == 1) {
+        const double s = ((((sm >> k) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
+        re *= s; im *= s;
+        if (((em >> k) | (em >> l)) & 1ull) { re = 0.0; im = 0.0; }
+      }
+      dst[(size_t)k * nd + l] = mk(re, im);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row-owner gather: one warp per CSR row sums the element-row contributions
+// through the precomputed entry -> slot-offset map (no atomics).
+// RAW: element buffer without signs/elimination (ComputeLocal output).
+// ---------------------------------------------------------------------------
+template <bool RAW>
+__global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__restrict__ ea,
+                         const uint16_t *__restrict__ off, const int *__restrict__ I,
+                         const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd,
+                         const unsigned char *__restrict__ ess,
+                         const double *__restrict__ sign, const int *__restrict__ dof,
+                         int eliminate, int maxrow, dcplx *__restrict__ vals) {
+  extern __shared__ dcplx sacc[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int r = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (r >= n) return;
+  dcplx *acc = sacc + (size_t)wib * maxrow;
+  const int rb = I[r], nr = I[r + 1] - rb;
+  for (int j = lane; j < nr; j += 32) acc[j] = mk(0.0, 0.0);
+  __syncwarp();
+  const bool row_ess = eliminate && ess[r];
+  const int p1 = ea_ptr[r + 1];
+  for (int pp = ea_ptr[r]; pp < p1; ++pp) {
+    const int id = ea[pp];
+    const dcplx *src = Ae + (size_t)id * nd;
+    const uint16_t *o = off + (size_t)pp * nd;
+    double sa = 1.0;
+    int ebase = 0;
+    if (RAW) { sa = sign[id]; ebase = (id / nd) * nd; }
+    for (int b = lane; b < nd; b += 32) {
+      dcplx v = src[b];
+      const int j = o[b];
+      if (RAW) {
+        const double s = sa * sign[ebase + b];
+        v.re *= s; v.im *= s;
+        if (eliminate && (row_ess || ess[dof[ebase + b]])) v = mk(0.0, 0.0);
+      }
+      acc[j].re += v.re;
+      acc[j].im += v.im;
+    }
+    __syncwarp();
+  }
+  if (row_ess && lane == 0) {
+    int lo = 0, hi = nr - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (Jc[rb + mid] < r) lo = mid + 1; else hi = mid;
+    }
+    acc[lo] = mk(1.0, 0.0);
+  }
+  __syncwarp();
+  for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
+}
+
+// ---------------------------------------------------------------------------
+// symbolic CSR on the device
+// ---------------------------------------------------------------------------
+__global__ void k_count_rows(long long total, const int *__restrict__ dof, int *__restrict__ cnt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) atomicAdd(cnt + dof[i], 1);
+}
+
+__global__ void k_fill_rows(long long total, const int *__restrict__ dof,
+                            const int *__restrict__ ptr, int *__restrict__ fill,
+                            int *__restrict__ ea) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) {
+    const int r = dof[i];
+    ea[ptr[r] + atomicAdd(fill + r, 1)] = (int)i;
+  }
+}
+
+__global__ void k_max_reduce(int n, const int *__restrict__ ptr, int diff, int *__restrict__ out) {
+  // diff != 0: max of ptr[i+1]-ptr[i]; else max of ptr[i]
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, diff ? ptr[i + 1] - ptr[i] : ptr[i]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// one warp per row.  PASS 1: sort the row's (element, row) list, count unique
+// columns.  PASS 2: write sorted unique columns and the slot offsets.
+// PASS 3: given columns (I/Jcol from the caller): offsets by binary search.
+template <int PASS>
+__global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
+                               const int *__restrict__ ea_ptr, int *__restrict__ ea,
+                               int cap, int *__restrict__ cnt, const int *__restrict__ I,
+                               int *__restrict__ Jc, uint16_t *__restrict__ off,
+                               int *__restrict__ err) {
+  extern __shared__ int sh[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int r = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (r >= n) return;
+  int *buf = sh + (size_t)wib * (cap + 64);
+  int *lst = buf + cap;  // up to 64 (element,row) ids
+  const int p0 = ea_ptr[r], m = ea_ptr[r + 1] - p0;
+  if (m > 64) { if (lane == 0) atomicExch(err, 2); return; }
+  if (PASS == 1) {
+    if (lane < m) lst[lane] = ea[p0 + lane];
+    if (lane + 32 < m) lst[lane + 32] = ea[p0 + lane + 32];
+    __syncwarp();
+    if (lane == 0) {  // insertion sort (m is small)
+      for (int a = 1; a < m; ++a) {
+        const int v = lst[a];
+        int b = a - 1;
+        while (b >= 0 && lst[b] > v) { lst[b + 1] = lst[b]; --b; }
+        lst[b + 1] = v;
+      }
+    }
+    __syncwarp();
+    if (lane < m) ea[p0 + lane] = lst[lane];
+    if (lane + 32 < m) ea[p0 + lane + 32] = lst[lane + 32];
+  } else {
+    if (lane < m) lst[lane] = ea[p0 + lane];
+    if (lane + 32 < m) lst[lane + 32] = ea[p0 + lane + 32];
+  }
+  __syncwarp();
+  const int tot = m * nd;
+  if (PASS == 3) {
+    const int rb = I[r], re = I[r + 1];
+    for (int i = lane; i < tot; i += 32) {
+      const int id = lst[i / nd];
+      const int col = dof[(size_t)(id / nd) * nd + (i % nd)];
+      int lo = rb, hi = re;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (Jc[mid] < col) lo = mid + 1; else hi = mid;
+      }
+      if (lo >= re || Jc[lo] != col) { atomicExch(err, 1); lo = rb; }
+      off[(size_t)p0 * nd + i] = (uint16_t)(lo - rb);
+    }
+    return;
+  }
+  for (int i = lane; i < cap; i += 32) {
+    int v = 0x7fffffff;
+    if (i < tot) {
+      const int id = lst[i / nd];
+      v = dof[(size_t)(id / nd) * nd + (i % nd)];
+    }
+    buf[i] = v;
+  }
+  __syncwarp();
+  // bitonic sort (ascending)
+  for (int k = 2; k <= cap; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < cap; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int a = buf[i], b = buf[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) { buf[i] = b; buf[ixj] = a; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // unique: count / compact (chunks of 32 with ballot prefix)
+  int base = 0;
+  const int rbase = PASS == 2 ? I[r] : 0;
+  for (int c0 = 0; c0 < cap; c0 += 32) {
+    const int i = c0 + lane;
+    const int v = buf[i];
+    const bool keep = v != 0x7fffffff && (i == 0 || buf[i - 1] != v);
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (PASS == 2 && keep) Jc[rbase + base + __popc(bal & ((1u << lane) - 1u))] = v;
+    base += __popc(bal);
+  }
+  if (PASS == 1) {
+    if (lane == 0) cnt[r] = base;
+    return;
+  }
+  __syncwarp();
+  // offsets: binary search of each candidate in the unique list (global)
+  const int nr = base;
+  for (int i = lane; i < tot; i += 32) {
+    const int id = lst[i / nd];
+    const int col = dof[(size_t)(id / nd) * nd + (i % nd)];
+    int lo = 0, hi = nr - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (Jc[rbase + mid] < col) lo = mid + 1; else hi = mid;
+    }
+    off[(size_t)p0 * nd + i] = (uint16_t)lo;
+  }
+}
+
+__global__ void k_essmask(int ne, int nd, const int *__restrict__ dof,
+                          const unsigned char *__restrict__ ess,
+                          unsigned long long *__restrict__ mask) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  unsigned long long m = 0ull;
+  for (int k = 0; k < nd; ++k)
+    if (ess[dof[(size_t)e * nd + k]]) m |= 1ull << k;
+  mask[e] = m;
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMV with fused residual partial norms (warp per row)
+// ---------------------------------------------------------------------------
+__global__ void k_spmv_resid(int n, const int *__restrict__ I, const int *__restrict__ Jc,
+                             const dcplx *__restrict__ vals, const dcplx *__restrict__ x,
+                             const dcplx *__restrict__ b, dcplx *__restrict__ y,
+                             double *__restrict__ partials) {
+  __shared__ double red[2][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int r = blockIdx.x * (blockDim.x >> 5) + wib;
+  double rn = 0.0, bn = 0.0;
+  if (r < n) {
+    double ar = 0.0, ai = 0.0;
+    for (int k = I[r] + lane; k < I[r + 1]; k += 32) {
+      const dcplx a = vals[k], xv = x[Jc[k]];
+      ar = fma(a.re, xv.re, ar); ar = fma(-a.im, xv.im, ar);
+      ai = fma(a.re, xv.im, ai); ai = fma(a.im, xv.re, ai);
+    }
+    for (int o = 16; o; o >>= 1) {
+      ar += __shfl_xor_sync(0xffffffffu, ar, o);
+      ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    if (lane == 0) {
+      if (y) y[r] = mk(ar, ai);
+      if (b) {
+        const dcplx bv = b[r];
+        const double dr = ar - bv.re, di = ai - bv.im;
+        rn = dr * dr + di * di;
+        bn = bv.re * bv.re + bv.im * bv.im;
+      }
+    }
+  }
+  if (!partials) return;
+  if (lane == 0) { red[0][wib] = rn; red[1][wib] = bn; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { s0 += red[0][w]; s1 += red[1][w]; }
+    partials[2 * blockIdx.x] = s0;
+    partials[2 * blockIdx.x + 1] = s1;
+  }
+}
+
+__global__ void k_sum_partials(int nblk, const double *__restrict__ partials,
+                               double *__restrict__ out) {
+  __shared__ double red[2][32];
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    s0 += partials[2 * i];
+    s1 += partials[2 * i + 1];
+  }
+  for (int o = 16; o; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { red[0][w] = s0; red[1][w] = s1; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { a += red[0][i]; c += red[1][i]; }
+    out[0] = a;
+    out[1] = c;
+  }
+}
+
+// host [re; im] halves <-> interleaved
+__global__ void k_split_to_cplx(int n, const double *__restrict__ h2n, dcplx *__restrict__ z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = mk(h2n[i], h2n[n + i]);
+}
+
+// ---------------------------------------------------------------------------
+// scattered-field RHS (ScatterSource, problem_common.inc:218-266)
+// ---------------------------------------------------------------------------
+struct SlabWaveD {
+  dcplx qA, qB;
+  double zA, zB;
+  dcplx A[3], B[3];
+};
+
+// one warp per source element; lanes over local dofs
+__global__ void k_rhs_elem(int nsrc, const int *__restrict__ list, int nd, int p, Rule rm,
+                           const double *__restrict__ J9, const double *__restrict__ Ji9,
+                           const double *__restrict__ detJ, const double *__restrict__ v0,
+                           const int *__restrict__ slab_of, const dcplx *__restrict__ delta,
+                           const SlabWaveD *__restrict__ waves, int n_slab, int n_parts,
+                           const int *__restrict__ col_of_part, int ncol, double k0,
+                           const unsigned *__restrict__ fopack, dcplx *__restrict__ be) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= nsrc) return;
+  const int e = list[i];
+  double J[9], Ji[9];
+  for (int t = 0; t < 9; ++t) { J[t] = J9[(size_t)e * 9 + t]; Ji[t] = Ji9[(size_t)e * 9 + t]; }
+  const double det = detJ[e];
+  const double x0[3] = {v0[(size_t)e * 3], v0[(size_t)e * 3 + 1], v0[(size_t)e * 3 + 2]};
+  const int slab = slab_of[e];
+  const dcplx fac = cscale(k0 * k0, delta[e]);
+  const unsigned fp = fopack ? fopack[e] : 0u;
+  for (int c = 0; c < ncol; ++c) {
+    for (int kb = 0; kb < nd; kb += 32) {
+      const int k = kb + lane;
+      double br = 0.0, bi = 0.0;
+      for (int q = 0; q < rm.nq; ++q) {
+        const double *xi = rm.ip + q * 3;
+        const double z = x0[2] + J[6] * xi[0] + J[7] * xi[1] + J[8] * xi[2];
+        dcplx ev[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+        for (int pi = 0; pi < n_parts; ++pi) {
+          if (col_of_part[pi] != c) continue;
+          const SlabWaveD &sw = waves[(size_t)pi * n_slab + slab];
+          // exp(i q (z - zA)) = exp(-Im(q) dz) (cos(Re(q) dz) + i sin(Re(q) dz))
+          const double da = z - sw.zA, db = z - sw.zB;
+          const double ma = exp(-sw.qA.im * da), mb = exp(-sw.qB.im * db);
+          double sa, ca, sb, cb;
+          sincos(sw.qA.re * da, &sa, &ca);
+          sincos(sw.qB.re * db, &sb, &cb);
+          const dcplx up = mk(ma * ca, ma * sa), dn = mk(mb * cb, mb * sb);
+          for (int d = 0; d < 3; ++d)
+            ev[d] = cadd(ev[d], cadd(cmul(sw.A[d], up), cmul(sw.B[d], dn)));
+        }
+        const double w = rm.w[q] * det;
+        if (k < nd) {
+          const double *rv = rm.v + ((size_t)q * nd + k) * 3;
+          for (int d = 0; d < 3; ++d) {
+            const double pv = rv[0] * Ji[0 * 3 + d] + rv[1] * Ji[1 * 3 + d] + rv[2] * Ji[2 * 3 + d];
+            const dcplx f = cmul(fac, ev[d]);
+            br += w * pv * f.re;
+            bi += w * pv * f.im;
+          }
+        }
+      }
+      // dual transform on the element vector: b <- M^T b on face pairs
+      const double obr = __shfl_xor_sync(0xffffffffu, br, 1);
+      const double obi = __shfl_xor_sync(0xffffffffu, bi, 1);
+      const int f = (p >= 2 && k < nd) ? face_of(k & ~1, p) : -1;
+      if (f >= 0) {
+        const double *T = c_tinv + 4 * ((fp >> (8 * f)) & 0xffu);
+        const int cp = k & 1;
+        const double own = T[2 * cp + cp], oth = T[2 * cp + (1 - cp)];
+        const double nr = own * br + oth * obr, ni = own * bi + oth * obi;
+        br = nr; bi = ni;
+      }
+      if (k < nd) be[((size_t)i * ncol + c) * nd + k] = mk(br, bi);
+    }
+  }
+}
+
+__global__ void k_rhs_gather(int n, const int *__restrict__ ea_ptr, const int *__restrict__ ea,
+                             int nd, const int *__restrict__ src_slot,
+                             const double *__restrict__ sign, const dcplx *__restrict__ be,
+                             int ncol, const unsigned char *__restrict__ ess, int eliminate,
+                             dcplx *__restrict__ b) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  for (int c = 0; c < ncol; ++c) {
+    double br = 0.0, bi = 0.0;
+    if (!(eliminate && ess[r])) {
+      for (int pp = ea_ptr[r]; pp < ea_ptr[r + 1]; ++pp) {
+        const int id = ea[pp];
+        const int e = id / nd, a = id - e * nd;
+        const int s = src_slot[e];
+        if (s < 0) continue;
+        const dcplx v = be[((size_t)s * ncol + c) * nd + a];
+        br += sign[id] * v.re;
+        bi += sign[id] * v.im;
+      }
+    }
+    b[(size_t)c * n + r] = mk(br, bi);
+  }
+}
+
+}  // namespace lfasm_dev

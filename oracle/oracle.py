@@ -1,0 +1,262 @@
+"""ORACLE -- test infrastructure, not product code.
+
+ctypes wrappers of the two CPU checkers built by oracle/Makefile:
+
+* ``_build/liboracle.so``: this repository's serial restatement of the
+  reference assembly path (oracle/lfasm_oracle.cpp);
+* ``_ref/libref_asm.so``: the reference's own reassembler and CUDA kernels
+  compiled from its sources (oracle/ref_shim/ref_asm.cu), present where the
+  reference tree was available at build time.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from pathlib import Path
+
+import numpy as np
+
+from lithofem_b200._abi import (AsmDataC, IncidentPartC, ProblemC, c_double_p, c_int_p,
+                                marshal, marshal_parts)
+from lithofem_b200.problem import Problem
+from lithofem_b200.space import AsmData
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "liboracle.so"
+REF_SO = HERE / "_ref" / "libref_asm.so"
+
+_orc = None
+_ref = None
+
+
+def orc() -> ct.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"{ORACLE_SO} missing: run `make -C oracle`")
+        L = ct.CDLL(os.fspath(ORACLE_SO))
+        A, P = ct.POINTER(AsmDataC), ct.POINTER(ProblemC)
+        L.orc_local.argtypes = [A, P, ct.c_int, ct.c_int, ct.c_int, c_double_p]
+        L.orc_local.restype = ct.c_int
+        L.orc_csr.argtypes = [A, c_int_p, c_int_p]
+        L.orc_csr.restype = ct.c_longlong
+        L.orc_assemble.argtypes = [A, P, c_int_p, c_int_p, c_int_p, ct.c_int, ct.c_int, c_double_p]
+        L.orc_assemble.restype = ct.c_int
+        L.orc_spmv.argtypes = [ct.c_int, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p,
+                               c_double_p]
+        L.orc_spmv.restype = ct.c_double
+        L.orc_rhs.argtypes = [A, P, ct.POINTER(IncidentPartC), ct.c_int, c_int_p, ct.c_int,
+                              c_int_p, ct.c_int, ct.c_int, c_double_p]
+        L.orc_rhs.restype = ct.c_int
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> ct.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise RuntimeError(f"{REF_SO} missing: the reference tree was not available to build it")
+        L = ct.CDLL(os.fspath(REF_SO))
+        d, i = c_double_p, c_int_p
+        L.ref_set_problem.argtypes = [ct.c_double] * 8 + [ct.c_int, ct.c_int, d, i, i, d]
+        L.ref_set_problem.restype = ct.c_int
+        L.ref_ctx_create.argtypes = ([ct.c_int] * 4 + [i, d, i, i, d, d, d, d] +
+                                     [ct.c_int, d, d, d, d] * 2)
+        L.ref_ctx_create.restype = ct.c_void_p
+        L.ref_ctx_destroy.argtypes = [ct.c_void_p]
+        L.ref_ctx_build_csr.argtypes = [ct.c_void_p]
+        L.ref_ctx_build_csr.restype = ct.c_longlong
+        L.ref_ctx_get_csr.argtypes = [ct.c_void_p, i, i]
+        L.ref_ctx_reassemble.argtypes = [ct.c_void_p, d, d]
+        L.ref_ctx_time_reassemble.argtypes = [ct.c_void_p]
+        L.ref_ctx_time_reassemble.restype = ct.c_double
+        L.ref_ctx_element.argtypes = [ct.c_void_p, ct.c_int, d]
+        L.ref_ctx_gpu_local.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, d, d]
+        L.ref_ctx_gpu_local.restype = ct.c_int
+        L.ref_ctx_gpu_global.argtypes = [ct.c_void_p, i, ct.c_int, ct.c_int, ct.c_int, d, d, d]
+        L.ref_ctx_gpu_global.restype = ct.c_int
+        _ref = L
+    return _ref
+
+
+# ---------------------------------------------------------------------------
+# restatement
+# ---------------------------------------------------------------------------
+
+def local(ad: AsmData, prob: Problem, mask_cc: int, mask_mass: int, te: bool) -> np.ndarray:
+    m = marshal(ad, prob)
+    out = np.empty(2 * ad.ne * ad.nd * ad.nd)
+    orc().orc_local(ct.byref(m.ad), ct.byref(m.prob), mask_cc, mask_mass, int(te),
+                    out.ctypes.data_as(c_double_p))
+    return out.view(np.complex128).reshape(ad.ne, ad.nd, ad.nd)
+
+
+def csr(ad: AsmData) -> tuple[np.ndarray, np.ndarray]:
+    m = marshal(ad, Problem(k0=1, lx=1, ly=1, z_min=0, z_max=1, pml_thick=1))
+    I = np.empty(ad.height + 1, dtype=np.int32)
+    nnz = orc().orc_csr(ct.byref(m.ad), I.ctypes.data_as(c_int_p), None)
+    J = np.empty(nnz, dtype=np.int32)
+    orc().orc_csr(ct.byref(m.ad), I.ctypes.data_as(c_int_p), J.ctypes.data_as(c_int_p))
+    return I, J
+
+
+def assemble(ad: AsmData, prob: Problem, I: np.ndarray, J: np.ndarray, ess,
+             eliminate: bool) -> np.ndarray:
+    m = marshal(ad, prob)
+    ess = np.ascontiguousarray(np.asarray(ess, dtype=np.int32))
+    vals = np.empty(2 * len(J))
+    rc = orc().orc_assemble(ct.byref(m.ad), ct.byref(m.prob), I.ctypes.data_as(c_int_p),
+                            J.ctypes.data_as(c_int_p), ess.ctypes.data_as(c_int_p), len(ess),
+                            int(eliminate), vals.ctypes.data_as(c_double_p))
+    if rc:
+        raise RuntimeError("oracle: CSR position missing")
+    return vals.view(np.complex128)
+
+
+def spmv(I, J, vals: np.ndarray, x: np.ndarray, b: np.ndarray | None = None):
+    vals = np.ascontiguousarray(vals, dtype=np.complex128)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.empty_like(x)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.complex128)
+    rel = orc().orc_spmv(len(I) - 1, np.ascontiguousarray(I, dtype=np.int32).ctypes.data_as(c_int_p),
+                         np.ascontiguousarray(J, dtype=np.int32).ctypes.data_as(c_int_p),
+                         vals.view(np.float64).ctypes.data_as(c_double_p),
+                         x.view(np.float64).ctypes.data_as(c_double_p),
+                         None if bb is None else bb.view(np.float64).ctypes.data_as(c_double_p),
+                         y.view(np.float64).ctypes.data_as(c_double_p))
+    return y, rel
+
+
+def rhs(ad: AsmData, prob: Problem, parts, col_of_part, ncol: int, ess, eliminate: bool):
+    m = marshal(ad, prob)
+    arr, keep = marshal_parts(parts)
+    cols = np.ascontiguousarray(np.asarray(col_of_part, dtype=np.int32))
+    ess = np.ascontiguousarray(np.asarray(ess, dtype=np.int32))
+    b = np.empty(2 * ad.height * ncol)
+    orc().orc_rhs(ct.byref(m.ad), ct.byref(m.prob), arr, len(parts), cols.ctypes.data_as(c_int_p),
+                  ncol, ess.ctypes.data_as(c_int_p), len(ess), int(eliminate),
+                  b.ctypes.data_as(c_double_p))
+    del keep
+    return b.view(np.complex128).reshape(ncol, ad.height)
+
+
+# ---------------------------------------------------------------------------
+# reference build
+# ---------------------------------------------------------------------------
+
+class RefContext:
+    """The reference's AsmData + global problem, filled from our extraction."""
+
+    def __init__(self, ad: AsmData, prob: Problem, elements: np.ndarray | None = None):
+        L = ref()
+        self._keep = []
+        k = self._keep.append
+        regs = prob.regions
+        eps = np.ascontiguousarray(np.array([[r.eps.real, r.eps.imag] for r in regs]).reshape(-1))
+        dl = np.ascontiguousarray(np.array([[r.delta_eps.real, r.delta_eps.imag] for r in regs]).reshape(-1))
+        kind = np.array([r.kind for r in regs], dtype=np.int32)
+        slab = np.array([r.slab for r in regs], dtype=np.int32)
+        L.ref_set_problem(prob.k0, prob.kx, prob.ky, prob.z_min, prob.z_max, prob.pml_thick,
+                          prob.pml_order, prob.pml_target, ad.p, len(regs),
+                          eps.ctypes.data_as(c_double_p), kind.ctypes.data_as(c_int_p),
+                          slab.ctypes.data_as(c_int_p), dl.ctypes.data_as(c_double_p))
+        nd = ad.nd
+        sel = np.arange(ad.ne) if elements is None else np.asarray(elements)
+        ne = len(sel)
+
+        def f(a, shape_per):
+            a = np.ascontiguousarray(np.asarray(a).reshape(ad.ne, shape_per)[sel].reshape(-1))
+            k(a)
+            return a
+
+        dof = f(ad.dof.astype(np.int32), nd)
+        sign = f(ad.sign, nd)
+        fo = f(ad.fo.astype(np.int32), 4) if ad.p >= 2 else np.zeros(4 * ne, dtype=np.int32)
+        k(fo)
+        attr = f(ad.attr.astype(np.int32), 1)
+        J = f(ad.J, 9)
+        Ji = f(ad.Jinv, 9)
+        det = f(ad.detJ, 1)
+        v0 = f(ad.v0, 3)
+
+        def rule(r):
+            arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (r.ip, r.w, r.vshape, r.curl)]
+            for a in arrs:
+                k(a)
+            return [r.nq] + [a.ctypes.data_as(c_double_p) for a in arrs]
+
+        self.ne, self.nd, self.height = ne, nd, ad.height
+        self.ctx = L.ref_ctx_create(ne, nd, ad.p, ad.height, dof.ctypes.data_as(c_int_p),
+                                    sign.ctypes.data_as(c_double_p), fo.ctypes.data_as(c_int_p),
+                                    attr.ctypes.data_as(c_int_p), J.ctypes.data_as(c_double_p),
+                                    Ji.ctypes.data_as(c_double_p), det.ctypes.data_as(c_double_p),
+                                    v0.ctypes.data_as(c_double_p), *rule(ad.rule_cc),
+                                    *rule(ad.rule_mass))
+        self.nnz = None
+
+    def build_csr(self):
+        L = ref()
+        self.nnz = int(L.ref_ctx_build_csr(self.ctx))
+        I = np.empty(self.height + 1, dtype=np.int32)
+        J = np.empty(self.nnz, dtype=np.int32)
+        L.ref_ctx_get_csr(self.ctx, I.ctypes.data_as(c_int_p), J.ctypes.data_as(c_int_p))
+        return I, J
+
+    def reassemble(self) -> np.ndarray:
+        if self.nnz is None:
+            self.build_csr()
+        re = np.empty(self.nnz)
+        im = np.empty(self.nnz)
+        ref().ref_ctx_reassemble(self.ctx, re.ctypes.data_as(c_double_p), im.ctypes.data_as(c_double_p))
+        return re + 1j * im
+
+    def time_reassemble(self) -> float:
+        if self.nnz is None:
+            self.build_csr()
+        return float(ref().ref_ctx_time_reassemble(self.ctx))
+
+    def element(self, e: int) -> np.ndarray:
+        out = np.empty(2 * self.nd * self.nd)
+        ref().ref_ctx_element(self.ctx, e, out.ctypes.data_as(c_double_p))
+        return out.view(np.complex128).reshape(self.nd, self.nd)
+
+    def gpu_local(self, mask_cc: int, mask_mass: int, te: bool):
+        out = np.empty(2 * self.ne * self.nd * self.nd)
+        ms = ct.c_double()
+        rc = ref().ref_ctx_gpu_local(self.ctx, mask_cc, mask_mass, int(te),
+                                     out.ctypes.data_as(c_double_p), ct.byref(ms))
+        if rc:
+            raise RuntimeError(f"reference GPU local failed ({rc})")
+        return out.view(np.complex128).reshape(self.ne, self.nd, self.nd), ms.value
+
+    def gpu_global(self, ess, eliminate: bool, iters: int = 1, download: bool = True):
+        if self.nnz is None:
+            self.build_csr()
+        ess = np.ascontiguousarray(np.asarray(ess, dtype=np.int32))
+        out = np.empty(2 * self.nnz) if download else None
+        ml, msc = ct.c_double(), ct.c_double()
+        rc = ref().ref_ctx_gpu_global(self.ctx, ess.ctypes.data_as(c_int_p), len(ess),
+                                      int(eliminate), iters,
+                                      None if out is None else out.ctypes.data_as(c_double_p),
+                                      ct.byref(ml), ct.byref(msc))
+        if rc:
+            raise RuntimeError(f"reference GPU global failed ({rc})")
+        vals = None if out is None else out.view(np.complex128)
+        return vals, ml.value, msc.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "ctx", None):
+                ref().ref_ctx_destroy(self.ctx)
+                self.ctx = None
+        except Exception:
+            pass

@@ -1,0 +1,222 @@
+// Test-infrastructure build of the REFERENCE assembly code, compiled from the
+// reference tree's own files (solver/problem_common.inc, asm_data.inc,
+// asm_gpu.inc; included, never copied) against mfem_shim.hpp, and exposed
+// through a small C API for the parity tests and the CPU baseline:
+//
+//   ref_set_problem       fills the reference's global `prob`
+//                         (Problem/Region, problem_common.inc:18-67)
+//   ref_ctx_create        builds the reference's AsmData (asm_data.inc:77-97)
+//                         from caller arrays (the MFEM extraction step is
+//                         replaced by the caller's own extraction)
+//   ref_ctx_build_csr     build_csr_symbolic   (asm_data.inc:178-210)
+//   ref_ctx_reassemble    reassemble_all       (asm_data.inc:374-402)
+//   ref_ctx_element       reassemble_element   (asm_data.inc:218-370)
+//   ref_ctx_gpu_local     AsmGpu::Init + ComputeLocal + DownloadLocal
+//   ref_ctx_gpu_global    AsmGpuGlobal::BuildGlobal + ScatterEliminate
+//
+// Built by oracle/Makefile into oracle/_ref/libref_asm.so.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mfem_shim.hpp"
+#include "thirdparty/json.hpp"
+
+using namespace mfem;
+using json = nlohmann::json;
+using C = std::complex<double>;
+
+namespace {
+#include "problem_common.inc"
+#include "asm_data.inc"
+#include "asm_gpu.inc"
+}  // namespace
+
+namespace {
+void fill_rule(AsmRefRule &r, int nq, int nd, const double *ip, const double *w,
+               const double *v, const double *c) {
+  r.nq = nq;
+  r.ip.assign(ip, ip + (size_t)nq * 3);
+  r.w.assign(w, w + nq);
+  r.vshape.assign(v, v + (size_t)nq * nd * 3);
+  r.curl.assign(c, c + (size_t)nq * nd * 3);
+}
+}  // namespace
+
+extern "C" {
+
+int ref_set_problem(double k0, double kx, double ky, double z_min, double z_max,
+                    double pml_thick, double pml_order, double pml_target, int order,
+                    int n_regions, const double *eps, const int *kind, const int *slab,
+                    const double *delta_eps) {
+  prob = Problem();
+  prob.k0 = k0;
+  prob.kx = kx;
+  prob.ky = ky;
+  prob.z_min = z_min;
+  prob.z_max = z_max;
+  prob.pml_thick = pml_thick;
+  prob.pml_order = pml_order;
+  prob.pml_target = pml_target;
+  prob.order = order;
+  for (int r = 0; r < n_regions; ++r) {
+    Region g;
+    g.eps = C(eps[2 * r], eps[2 * r + 1]);
+    g.slab = slab[r];
+    g.is_frustum = kind[r] == 1;
+    g.is_pml = kind[r] == 2 || kind[r] == 3;
+    g.pml_top = kind[r] == 3;
+    g.delta_eps = C(delta_eps[2 * r], delta_eps[2 * r + 1]);
+    prob.regions.push_back(g);
+  }
+  return 0;
+}
+
+void *ref_ctx_create(int ne, int nd, int p, int height, const int *dof, const double *sign,
+                     const int *fo, const int *attr, const double *J, const double *Jinv,
+                     const double *detJ, const double *v0, int nq_cc, const double *ip_cc,
+                     const double *w_cc, const double *v_cc, const double *c_cc, int nq_m,
+                     const double *ip_m, const double *w_m, const double *v_m,
+                     const double *c_m) {
+  AsmData *ad = new AsmData();
+  ad->ne = ne;
+  ad->nd = nd;
+  ad->p = p;
+  ad->height = height;
+  ad->has_kpar = prob.kx != 0.0 || prob.ky != 0.0;
+  const size_t nen = (size_t)ne * nd;
+  ad->dof.assign(dof, dof + nen);
+  ad->sign.assign(sign, sign + nen);
+  if (p >= 2) ad->fo.assign(fo, fo + (size_t)ne * 4);
+  ad->attr.assign(attr, attr + ne);
+  ad->J.assign(J, J + (size_t)ne * 9);
+  ad->Jinv.assign(Jinv, Jinv + (size_t)ne * 9);
+  ad->detJ.assign(detJ, detJ + ne);
+  ad->v0.assign(v0, v0 + (size_t)ne * 3);
+  fill_rule(ad->rule_cc, nq_cc, nd, ip_cc, w_cc, v_cc, c_cc);
+  fill_rule(ad->rule_mass, nq_m, nd, ip_m, w_m, v_m, c_m);
+  return ad;
+}
+
+void ref_ctx_destroy(void *ctx) { delete static_cast<AsmData *>(ctx); }
+
+long long ref_ctx_build_csr(void *ctx) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  build_csr_symbolic(*ad);
+  return (long long)ad->Jcol.size();
+}
+
+int ref_ctx_get_csr(void *ctx, int *I, int *J) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  std::copy(ad->I.begin(), ad->I.end(), I);
+  std::copy(ad->Jcol.begin(), ad->Jcol.end(), J);
+  return 0;
+}
+
+int ref_ctx_reassemble(void *ctx, double *vre, double *vim) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  std::vector<double> re, im;
+  reassemble_all(*ad, re, im);
+  std::copy(re.begin(), re.end(), vre);
+  std::copy(im.begin(), im.end(), vim);
+  return 0;
+}
+
+// reassemble_all on the context, output discarded; returns seconds
+double ref_ctx_time_reassemble(void *ctx) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  std::vector<double> re, im;
+  const auto t0 = std::chrono::steady_clock::now();
+  reassemble_all(*ad, re, im);
+  const auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+int ref_ctx_element(void *ctx, int e, double *out) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  std::vector<C> Ae;
+  reassemble_element(*ad, e, Ae);
+  for (size_t i = 0; i < Ae.size(); ++i) {
+    out[2 * i] = Ae[i].real();
+    out[2 * i + 1] = Ae[i].imag();
+  }
+  return 0;
+}
+
+int ref_ctx_gpu_local(void *ctx, int mask_cc, int mask_mass, int te, double *out, double *ms) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  AsmGpu g;
+  if (!g.Init(*ad, 0)) return 1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a);
+  if (!g.ComputeLocal(mask_cc, mask_mass, te != 0)) return 2;
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, a, b);
+  if (ms) *ms = t;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::vector<DC> h;
+  if (out) {
+    if (!g.DownloadLocal(h)) return 3;
+    std::memcpy(out, h.data(), h.size() * sizeof(DC));
+  }
+  return 0;
+}
+
+// Full reference GPU path: ComputeLocal(CC, MASS[|kpar terms], te) +
+// ScatterEliminate, repeated `iters` times after one warm-up; ms_* are the
+// per-iteration averages of the two stages.
+int ref_ctx_gpu_global(void *ctx, const int *ess, int n_ess, int eliminate, int iters,
+                       double *vals_out, double *ms_local, double *ms_scatter) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  if (ad->Jcol.empty()) build_csr_symbolic(*ad);
+  Array<int> ess_list;
+  for (int i = 0; i < n_ess; ++i) ess_list.Append(ess[i]);
+  AsmGpuGlobal g;
+  if (!g.Init(*ad, 0)) return 1;
+  if (!g.BuildGlobal(*ad, ess_list)) return 2;
+  const bool kpar = prob.kx != 0.0 || prob.ky != 0.0;
+  const int mm = ASM_MASS | (kpar ? ASM_CROSS0 | ASM_CROSS1 | ASM_KLK : 0);
+  cudaEvent_t a, b, c;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventCreate(&c);
+  double tl = 0.0, ts = 0.0;
+  for (int it = -1; it < std::max(iters, 1); ++it) {
+    cudaEventRecord(a);
+    if (!g.ComputeLocal(ASM_CURLCURL, mm, true)) return 3;
+    cudaEventRecord(b);
+    if (!g.ScatterEliminate(eliminate != 0)) return 4;
+    cudaEventRecord(c);
+    cudaEventSynchronize(c);
+    float t1 = 0.f, t2 = 0.f;
+    cudaEventElapsedTime(&t1, a, b);
+    cudaEventElapsedTime(&t2, b, c);
+    if (it >= 0) { tl += t1; ts += t2; }
+  }
+  const int n_it = std::max(iters, 1);
+  if (ms_local) *ms_local = tl / n_it;
+  if (ms_scatter) *ms_scatter = ts / n_it;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaEventDestroy(c);
+  if (vals_out) {
+    std::vector<DC> h;
+    if (!g.DownloadValues(h)) return 5;
+    std::memcpy(vals_out, h.data(), h.size() * sizeof(DC));
+  }
+  return 0;
+}
+
+}  // extern "C"
