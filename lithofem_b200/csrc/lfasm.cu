@@ -84,6 +84,7 @@ struct lfasm_handle {
   int async_mode = 0;
   int ne = 0, nd = 0, p = 0, n = 0, has_kpar = 0;
   int ndp = 0, ndp4 = 0;
+  int sm_count = 148;
   long long nnz = 0;
   // element data
   int *dof = nullptr;
@@ -422,7 +423,11 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
     LF_CUDA_H(upload(h->src_slot, slot.data(), ne));
   }
 
-  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * nd * sizeof(dcplx)));
+  // element buffer: dense nd x nd rows for lfasm_compute_local, padded row
+  // stride ndp (even) for the fused path so every row starts on a 32-byte
+  // sector and column pairs fill whole sectors
+  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * h->ndp * sizeof(dcplx)));
+  LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
   LF_CUDA_H(cudaDeviceSynchronize());
 #undef LF_CUDA_H
   *out = h;
@@ -448,6 +453,31 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
   return LFASM_OK;
 }
 
+}  // extern "C"
+
+template <int NDP8>
+static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int mask_mass, int te,
+                      int eliminate, int rs) {
+  const size_t smem = PmlShape<NDP8>::SMEM;
+  const int threads = NDP8 * 4;
+  auto go = [&](auto kern) -> int {
+    LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    LF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    const int grid = std::max(1, std::min(h->n_pml, std::max(per_sm, 1) * h->sm_count));
+    kern<<<grid, threads, smem, h->stream>>>(
+        h->n_pml, h->pml_list, h->nd, rs, h->p, h->rcc.view(), h->rm.view(), h->J, h->Jinv,
+        h->detJ, h->v0, h->attr, h->eps_tab, h->elem_eps, h->pml, mask_cc, mask_mass, te,
+        eliminate, h->fopack, h->signmask, h->essmask, h->Ae);
+    LF_LAUNCHED();
+    return LFASM_OK;
+  };
+  if (cross) return mode ? go(k_pml_mma<NDP8, true, 1>) : go(k_pml_mma<NDP8, true, 0>);
+  return mode ? go(k_pml_mma<NDP8, false, 1>) : go(k_pml_mma<NDP8, false, 0>);
+}
+
+extern "C" {
+
 static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int mode,
                         int eliminate) {
   if ((mask_cc & ~LFASM_CURLCURL) || (mask_mass & LFASM_CURLCURL) || (mask_mass & ~31))
@@ -459,19 +489,23 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
   const bool prof = mode == 1 && h->profile;
   // every element is written by exactly one of the two paths: no memset
   if (prof) LF_CUDA(cudaEventRecord(h->ev[0], h->stream));
+  const int rs = mode ? h->ndp : h->nd;
   if (h->n_bulk) {
     const int nb = h->n_bulk;
     k_prep_bulk<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
                                                          h->detJ, h->attr, h->eps_tab,
                                                          h->elem_eps, h->pml, mask, h->rec);
     LF_LAUNCHED();
-    const int chunk = 16;
     const int ytiles = ((h->ndp / 2) * h->ndp + BULK_THREADS - 1) / BULK_THREADS;
+    // about two waves of resident blocks; each block keeps its S-table
+    // values in registers across its chunk of elements
+    const long long want = (long long)h->sm_count * 8;
+    int chunk = (int)std::max<long long>(16, ((long long)nb * ytiles + want - 1) / want);
     dim3 grid((nb + chunk - 1) / chunk, ytiles);
 #define LF_BULK(C, M)                                                             \
   k_bulk<C, M><<<grid, BULK_THREADS, 0, h->stream>>>(                             \
       nb, h->bulk_list, h->rec, h->S, h->nd, h->ndp, h->p, chunk, te, eliminate,  \
-      h->fopack, h->signmask, h->essmask, h->Ae)
+      rs, h->fopack, h->signmask, h->essmask, h->Ae)
     if (cross) { if (mode) LF_BULK(true, 1); else LF_BULK(true, 0); }
     else { if (mode) LF_BULK(false, 1); else LF_BULK(false, 0); }
 #undef LF_BULK
@@ -479,25 +513,10 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[1], h->stream));
   if (h->n_pml) {
-    const int tpr = h->ndp4 / 4;
-    const int threads = ((tpr * tpr + 31) / 32) * 32;
-    const size_t smem = (size_t)PML_QC * 6 * h->ndp4 * (sizeof(double) + sizeof(dcplx)) +
-                        PML_QC * sizeof(QCoef);
-#define LF_PML(C, M)                                                                 \
-  do {                                                                               \
-    LF_CUDA(cudaFuncSetAttribute(k_pml<C, M>,                                        \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                                 (int)smem));                                        \
-    k_pml<C, M><<<h->n_pml, threads, smem, h->stream>>>(                             \
-        h->n_pml, h->pml_list, h->nd, h->ndp4, h->p, h->rcc.view(), h->rm.view(),    \
-        h->J, h->Jinv, h->detJ, h->v0, h->attr, h->eps_tab, h->elem_eps, h->pml,     \
-        mask_cc, mask_mass, te, eliminate, h->fopack, h->signmask, h->essmask,       \
-        h->Ae);                                                                      \
-  } while (0)
-    if (cross) { if (mode) LF_PML(true, 1); else LF_PML(true, 0); }
-    else { if (mode) LF_PML(false, 1); else LF_PML(false, 0); }
-#undef LF_PML
-    LF_LAUNCHED();
+    int rc = h->p == 1 ? launch_pml<8>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs)
+           : h->p == 2 ? launch_pml<24>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs)
+                       : launch_pml<48>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs);
+    if (rc) return rc;
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[2], h->stream));
   return LFASM_OK;
@@ -664,12 +683,12 @@ static int gather(lfasm_handle *h, bool raw, int eliminate) {
   if (raw) {
     LF_CUDA(cudaFuncSetAttribute(k_gather<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_gather<true><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
-                                                      h->Ae, h->nd, h->ess, h->sign, h->dof,
+                                                      h->Ae, h->nd, h->nd, h->ess, h->sign, h->dof,
                                                       eliminate, h->max_row, h->vals);
   } else {
     LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_gather<false><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
-                                                       h->Ae, h->nd, h->ess, h->sign, h->dof,
+                                                       h->Ae, h->nd, h->ndp, h->ess, h->sign, h->dof,
                                                        eliminate, h->max_row, h->vals);
   }
   LF_LAUNCHED();

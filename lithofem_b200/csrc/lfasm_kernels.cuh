@@ -14,7 +14,7 @@
 //    and exact for these polynomial integrands;
 //  * PML elements: per-quadrature-point contraction A += X_q^T (W_q X_q)
 //    with X_q the (face-transformed) physical shapes and W_q the complex
-//    coefficient tensors, register-tiled over 4x4 entry blocks.
+//    coefficient tensors, on FP64 tensor cores (mma.sync m8n8k4 .f64).
 
 #pragma once
 
@@ -41,7 +41,6 @@ constexpr int REC = 40;        // doubles per bulk-element coefficient record
 constexpr int NT_CC = 6;       // symmetric (j <= j') pairs
 constexpr int NT_ALL = 30;     // 6 cc + 6 vv + 9 vc + 9 cv
 constexpr int BULK_THREADS = 128;
-constexpr int MAXND = 48;
 
 __constant__ double c_tinv[24];   // 2x2 column-major blocks per orientation
 
@@ -148,7 +147,7 @@ template <bool CROSS, int MODE>
 __global__ void __launch_bounds__(BULK_THREADS)
 k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
        const double *__restrict__ S, int nd, int ndp, int p, int chunk, int te,
-       int eliminate, const unsigned *__restrict__ fopack,
+       int eliminate, int rs, const unsigned *__restrict__ fopack,
        const unsigned long long *__restrict__ signmask,
        const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
   constexpr int NT = CROSS ? NT_ALL : 12;
@@ -232,226 +231,261 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
       }
     }
     if (valid && l < nd) {
-      dcplx *dst = Ae + (size_t)e * nd * nd;
-      dst[(size_t)r0 * nd + l] = mk(re0, im0);
-      if (r1 < nd) dst[(size_t)r1 * nd + l] = mk(re1, im1);
+      dcplx *dst = Ae + (size_t)e * nd * rs;
+      dst[(size_t)r0 * rs + l] = mk(re0, im0);
+      if (r1 < nd) dst[(size_t)r1 * rs + l] = mk(re1, im1);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// PML element kernel: one element per block, thread <-> 4x4 entry tile.
+// PML element kernel on FP64 tensor cores (mma.sync m8n8k4 .f64, DMMA).
+//
+// Per element: A_e = sum_r X[r]^T Y[r] over the staged rows r (3 curl rows
+// per cc-rule point; 3 shape rows, plus 3 curl rows when the k-parallel
+// cross terms are on, per mass-rule point), X real, Y = W X complex kept as
+// two real planes.  As a GEMM: C (M x N) = A (M x K) B (K x N) with
+// A[m][r] = X[r][m], B[r][n] = Yre/Yim[r][n]; M = N = NDP8 (nd rounded up
+// to 8).  One warp per 8-column tile (real and imaginary planes), all
+// M tiles, so the epilogue holds both parts of each entry.  Rows are staged
+// in chunks of PML_QC points; blocks are persistent over the PML elements.
 // ---------------------------------------------------------------------------
 constexpr int PML_QC = 8;  // quadrature points staged per round
 
 struct QCoef {  // per quadrature point, already multiplied by w_q detJ
-  dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries
+  dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries (cc rule: Lambda^-1 diagonal)
   dcplx b02, b12, b20, b21;           // M0 = i K Lambda^-1
   dcplx c02, c12, c20, c21;           // M1 = i Lambda^-1 K
 };
 
-template <bool CROSS, int MODE>
-__global__ void k_pml(int npml, const int *__restrict__ list, int nd, int ndp4, int p,
-                      Rule rcc, Rule rm, const double *__restrict__ J9,
-                      const double *__restrict__ Ji9, const double *__restrict__ detJ,
-                      const double *__restrict__ v0, const int *__restrict__ attr,
-                      const dcplx *__restrict__ eps_tab, const dcplx *__restrict__ elem_eps,
-                      PmlParams pml, int mask_cc, int mask_mass, int te, int eliminate,
-                      const unsigned *__restrict__ fopack,
-                      const unsigned long long *__restrict__ signmask,
-                      const unsigned long long *__restrict__ essmask,
-                      dcplx *__restrict__ Ae) {
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int NDP8>
+struct PmlShape {
+  static constexpr int NW = NDP8 / 8;                    // warps = column tiles
+  static constexpr int MT = NDP8 / 8;                    // row tiles
+  static constexpr int LD = (NDP8 % 16 == 0) ? NDP8 + 8 : NDP8;  // row stride = 8 mod 16
+  static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
+  static constexpr size_t SMEM = (size_t)3 * RMAX * LD * sizeof(double) + PML_QC * sizeof(QCoef);
+};
+
+template <int NDP8, bool CROSS, int MODE>
+__global__ void __launch_bounds__(NDP8 * 4)
+k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
+          const double *__restrict__ J9, const double *__restrict__ Ji9,
+          const double *__restrict__ detJ, const double *__restrict__ v0,
+          const int *__restrict__ attr, const dcplx *__restrict__ eps_tab,
+          const dcplx *__restrict__ elem_eps, PmlParams pml, int mask_cc, int mask_mass,
+          int te, int eliminate, const unsigned *__restrict__ fopack,
+          const unsigned long long *__restrict__ signmask,
+          const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
+  using Sh = PmlShape<NDP8>;
+  constexpr int LD = Sh::LD, MT = Sh::MT, RMAX = Sh::RMAX;
   extern __shared__ double smem[];
-  const int rows_q = CROSS ? 6 : 3;
-  const int maxrows = PML_QC * 6;
-  double *Xs = smem;                                    // maxrows * ndp4
-  dcplx *Ys = reinterpret_cast<dcplx *>(Xs + (size_t)maxrows * ndp4);  // maxrows*ndp4
-  QCoef *qc = reinterpret_cast<QCoef *>(Ys + (size_t)maxrows * ndp4); // PML_QC
+  double *Xs = smem;
+  double *Yr = Xs + RMAX * LD;
+  double *Yi = Yr + RMAX * LD;
+  QCoef *qc = reinterpret_cast<QCoef *>(Yi + RMAX * LD);
   __shared__ double sJ[9], sJi[9], sdet, sv0z;
   __shared__ dcplx seps;
   __shared__ unsigned sfo;
 
-  const int e = list[blockIdx.x];
-  const int tid = threadIdx.x;
-  if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
-  if (tid == 0) {
-    sdet = detJ[e];
-    sv0z = v0[(size_t)e * 3 + 2];
-    seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
-    sfo = fopack[e];
-  }
-  __syncthreads();
-
-  const int tpr = ndp4 >> 2;               // tiles per row
-  const int ntile = tpr * tpr;
-  const bool active = tid < ntile;
-  const int ti = active ? tid / tpr : 0, tl = active ? tid - ti * tpr : 0;
-  double acc_re[4][4], acc_im[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) { acc_re[a][b] = 0.0; acc_im[a][b] = 0.0; }
-
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
   const double k2 = pml.k0 * pml.k0;
   const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
-  const int npair = ndp4 >> 1;
+  constexpr int npair = NDP8 / 2;
 
-  for (int rule = 0; rule < 2; ++rule) {
-    const int mask = rule == 0 ? mask_cc : mask_mass;
-    if (!mask) continue;
-    const Rule R = rule == 0 ? rcc : rm;
-    const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
-    const bool need_v = rule == 1;
-    const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
-    (void)rows_q;
-    for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
-      const int nqc = min(PML_QC, R.nq - q0);
-      // per-point coefficients
-      if (tid < nqc) {
-        const int q = q0 + tid;
-        const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
-                         sJ[8] * R.ip[q * 3 + 2];
-        const dcplx s = pml_s(pml, z);
-        const dcplx si = cinv(s);
-        const double w = R.w[q] * sdet;
-        QCoef c;
-        if (rule == 0) {
-          // cc: a00 = w li0, a11 = w li1, a22 = w li2 (diagonal), rest unused
-          c.a00 = cscale(w, si); c.a11 = cscale(w, si); c.a22 = cscale(w, s);
-          c.a01 = mk(0, 0); c.a10 = mk(0, 0);
-          c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
-        } else {
-          const dcplx li0 = si, li1 = si, li2 = s;
-          dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
-          if (mask & 2) {
-            const dcplx me = cscale(-k2, seps);
-            a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
-          }
-          if (mask & 16) {
-            a00 = cadd(a00, cscale(-K02 * K20, li2));
-            a01 = cadd(a01, cscale(-K02 * K21, li2));
-            a10 = cadd(a10, cscale(-K12 * K20, li2));
-            a11 = cadd(a11, cscale(-K12 * K21, li2));
-            a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
-          }
-          c.a00 = cscale(w, a00); c.a01 = cscale(w, a01); c.a10 = cscale(w, a10);
-          c.a11 = cscale(w, a11); c.a22 = cscale(w, a22);
-          const dcplx iu = mk(0.0, 1.0);
-          if (mask & 4) {
-            c.b02 = cscale(w * K02, cmul(iu, li2)); c.b12 = cscale(w * K12, cmul(iu, li2));
-            c.b20 = cscale(w * K20, cmul(iu, li0)); c.b21 = cscale(w * K21, cmul(iu, li1));
-          } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
-          if (mask & 8) {
-            c.c02 = cscale(w * K02, cmul(iu, li0)); c.c12 = cscale(w * K12, cmul(iu, li1));
-            c.c20 = cscale(w * K20, cmul(iu, li2)); c.c21 = cscale(w * K21, cmul(iu, li2));
-          } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
-        }
-        qc[tid] = c;
-      }
-      __syncthreads();
-      // stage X (transformed physical shapes) and Y = W X, column pairs
-      for (int it = tid; it < nqc * npair; it += blockDim.x) {
-        const int qi = it / npair, pr = it - qi * npair;
-        const int q = q0 + qi;
-        double v[2][3], c[2][3];
-        for (int h = 0; h < 2; ++h) {
-          const int k = 2 * pr + h;
-          for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
-          if (k < nd) {
-            const double *rv = R.v + ((size_t)q * nd + k) * 3;
-            const double *rc = R.c + ((size_t)q * nd + k) * 3;
-            for (int d = 0; d < 3; ++d) {
-              if (need_v)
-                v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
-              if (need_c)
-                c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
-            }
-          }
-        }
-        if (te && p >= 2) {
-          const int f = face_of(2 * pr, p);
-          if (f >= 0) {
-            const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
-            for (int d = 0; d < 3; ++d) {
-              const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
-              v[0][d] = v0_ * T[0] + v1_ * T[1];
-              v[1][d] = v0_ * T[2] + v1_ * T[3];
-              c[0][d] = c0_ * T[0] + c1_ * T[1];
-              c[1][d] = c0_ * T[2] + c1_ * T[3];
-            }
-          }
-        }
-        const QCoef &C = qc[qi];
-        for (int h = 0; h < 2; ++h) {
-          const int k = 2 * pr + h;
-          const int rb = qi * rq;
-          if (rule == 0) {
-            for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + d) * ndp4 + k] = c[h][d];
-            Ys[(size_t)(rb + 0) * ndp4 + k] = cscale(c[h][0], C.a00);
-            Ys[(size_t)(rb + 1) * ndp4 + k] = cscale(c[h][1], C.a11);
-            Ys[(size_t)(rb + 2) * ndp4 + k] = cscale(c[h][2], C.a22);
-          } else {
-            for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + d) * ndp4 + k] = v[h][d];
-            const double *vv = v[h], *cc = c[h];
-            dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
-            dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
-            dcplx y2 = cscale(vv[2], C.a22);
-            if (need_c) {
-              y0 = cadd(y0, cscale(cc[2], C.b02));
-              y1 = cadd(y1, cscale(cc[2], C.b12));
-              y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
-              for (int d = 0; d < 3; ++d) Xs[(size_t)(rb + 3 + d) * ndp4 + k] = cc[d];
-              Ys[(size_t)(rb + 3) * ndp4 + k] = cscale(vv[2], C.c02);
-              Ys[(size_t)(rb + 4) * ndp4 + k] = cscale(vv[2], C.c12);
-              Ys[(size_t)(rb + 5) * ndp4 + k] = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
-            }
-            Ys[(size_t)(rb + 0) * ndp4 + k] = y0;
-            Ys[(size_t)(rb + 1) * ndp4 + k] = y1;
-            Ys[(size_t)(rb + 2) * ndp4 + k] = y2;
-          }
-        }
-      }
-      __syncthreads();
-      if (active) {
-        const int nrows = nqc * rq;
-        for (int r = 0; r < nrows; ++r) {
-          const double *xr = Xs + (size_t)r * ndp4 + 4 * ti;
-          const dcplx *yr = Ys + (size_t)r * ndp4 + 4 * tl;
-          double x[4];
-          dcplx y[4];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) { x[a] = xr[a]; y[a] = yr[a]; }
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-              acc_re[a][b] = fma(x[a], y[b].re, acc_re[a][b]);
-              acc_im[a][b] = fma(x[a], y[b].im, acc_im[a][b]);
-            }
-        }
-      }
-      __syncthreads();
+  for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
+    const int e = list[ie];
+    __syncthreads();  // previous element done with the shared scalars
+    if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
+    if (tid == 0) {
+      sdet = detJ[e];
+      sv0z = v0[(size_t)e * 3 + 2];
+      seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+      sfo = fopack[e];
     }
-  }
-  if (!active) return;
-  const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
-  const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
-  dcplx *dst = Ae + (size_t)e * nd * nd;
+    double cr[MT][2], ci[MT][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int k = 4 * ti + a;
-    if (k >= nd) continue;
+    for (int m = 0; m < MT; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
+    __syncthreads();
+
+    for (int rule = 0; rule < 2; ++rule) {
+      const int mask = rule == 0 ? mask_cc : mask_mass;
+      if (!mask) continue;
+      const Rule R = rule == 0 ? rcc : rm;
+      const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+      const bool need_v = rule == 1;
+      const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+      for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
+        const int nqc = min(PML_QC, R.nq - q0);
+        const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
+        if (tid < nqc) {
+          const int q = q0 + tid;
+          const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
+                           sJ[8] * R.ip[q * 3 + 2];
+          const dcplx s = pml_s(pml, z);
+          const dcplx si = cinv(s);
+          const double wq = R.w[q] * sdet;
+          QCoef c;
+          if (rule == 0) {
+            c.a00 = cscale(wq, si); c.a11 = cscale(wq, si); c.a22 = cscale(wq, s);
+            c.a01 = mk(0, 0); c.a10 = mk(0, 0);
+            c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
+          } else {
+            const dcplx li0 = si, li1 = si, li2 = s;
+            dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
+            if (mask & 2) {
+              const dcplx me = cscale(-k2, seps);
+              a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
+            }
+            if (mask & 16) {
+              a00 = cadd(a00, cscale(-K02 * K20, li2));
+              a01 = cadd(a01, cscale(-K02 * K21, li2));
+              a10 = cadd(a10, cscale(-K12 * K20, li2));
+              a11 = cadd(a11, cscale(-K12 * K21, li2));
+              a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
+            }
+            c.a00 = cscale(wq, a00); c.a01 = cscale(wq, a01); c.a10 = cscale(wq, a10);
+            c.a11 = cscale(wq, a11); c.a22 = cscale(wq, a22);
+            const dcplx iu = mk(0.0, 1.0);
+            if (mask & 4) {
+              c.b02 = cscale(wq * K02, cmul(iu, li2)); c.b12 = cscale(wq * K12, cmul(iu, li2));
+              c.b20 = cscale(wq * K20, cmul(iu, li0)); c.b21 = cscale(wq * K21, cmul(iu, li1));
+            } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
+            if (mask & 8) {
+              c.c02 = cscale(wq * K02, cmul(iu, li0)); c.c12 = cscale(wq * K12, cmul(iu, li1));
+              c.c20 = cscale(wq * K20, cmul(iu, li2)); c.c21 = cscale(wq * K21, cmul(iu, li2));
+            } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
+          }
+          qc[tid] = c;
+        }
+        // zero the padding rows up to a multiple of 4
+        for (int i = tid; i < (nrows4 - nrows) * LD; i += blockDim.x) {
+          const int r = nrows + i / LD, k = i % LD;
+          Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+        }
+        __syncthreads();
+        for (int it = tid; it < nqc * npair; it += blockDim.x) {
+          const int qi = it / npair, pr = it - qi * npair;
+          const int q = q0 + qi;
+          double v[2][3], c[2][3];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int l = 4 * tl + b;
-      if (l >= nd) continue;
-      double re = acc_re[a][b], im = acc_im[a][b];
-      if (MODE == 1) {
-        const double s = ((((sm >> k) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
-        re *= s; im *= s;
-        if (((em >> k) | (em >> l)) & 1ull) { re = 0.0; im = 0.0; }
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * pr + h;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
+            if (k < nd) {
+              const double *rv = R.v + ((size_t)q * nd + k) * 3;
+              const double *rc = R.c + ((size_t)q * nd + k) * 3;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                if (need_v)
+                  v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
+                if (need_c)
+                  c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
+              }
+            }
+          }
+          if (te && p >= 2) {
+            const int f = face_of(2 * pr, p);
+            if (f >= 0) {
+              const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
+                v[0][d] = v0_ * T[0] + v1_ * T[1];
+                v[1][d] = v0_ * T[2] + v1_ * T[3];
+                c[0][d] = c0_ * T[0] + c1_ * T[1];
+                c[1][d] = c0_ * T[2] + c1_ * T[3];
+              }
+            }
+          }
+          const QCoef &C = qc[qi];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * pr + h;
+            const int rb = qi * rq;
+            if (rule == 0) {
+#pragma unroll
+              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
+              const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
+                          y2 = cscale(c[h][2], C.a22);
+              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+            } else {
+              const double *vv = v[h], *cc = c[h];
+#pragma unroll
+              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
+              dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+              dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+              dcplx y2 = cscale(vv[2], C.a22);
+              if (need_c) {
+                y0 = cadd(y0, cscale(cc[2], C.b02));
+                y1 = cadd(y1, cscale(cc[2], C.b12));
+                y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
+                const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
+                            z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+                Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
+                Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
+                Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
+              }
+              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+            }
+          }
+        }
+        __syncthreads();
+        // tensor-core contraction of the staged rows
+        for (int r0 = 0; r0 < nrows4; r0 += 4) {
+          const double br = Yr[(r0 + t4) * LD + w * 8 + g];
+          const double bi = Yi[(r0 + t4) * LD + w * 8 + g];
+#pragma unroll
+          for (int m = 0; m < MT; ++m) {
+            const double a = Xs[(r0 + t4) * LD + m * 8 + g];
+            dmma(cr[m][0], cr[m][1], a, br);
+            dmma(ci[m][0], ci[m][1], a, bi);
+          }
+        }
+        __syncthreads();
       }
-      dst[(size_t)k * nd + l] = mk(re, im);
+    }
+    // epilogue: C[row = m*8 + g][col = w*8 + 2*t4 + i]
+    const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
+    const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+    dcplx *dst = Ae + (size_t)e * nd * rs;
+    const int col = w * 8 + 2 * t4;
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+      const int row = m * 8 + g;
+      if (row >= nd) continue;
+      dcplx v2[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int l = col + i;
+        double re = cr[m][i], im = ci[m][i];
+        if (MODE == 1) {
+          const double sg = ((((sm >> row) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
+          re *= sg; im *= sg;
+          if (((em >> row) | (em >> l)) & 1ull) { re = 0.0; im = 0.0; }
+        }
+        v2[i] = mk(re, im);
+      }
+      if (col + 1 < nd) {
+        dst[(size_t)row * rs + col] = v2[0];
+        dst[(size_t)row * rs + col + 1] = v2[1];
+      } else if (col < nd) {
+        dst[(size_t)row * rs + col] = v2[0];
+      }
     }
   }
 }
@@ -464,7 +498,7 @@ __global__ void k_pml(int npml, const int *__restrict__ list, int nd, int ndp4, 
 template <bool RAW>
 __global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__restrict__ ea,
                          const uint16_t *__restrict__ off, const int *__restrict__ I,
-                         const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd,
+                         const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd, int rs,
                          const unsigned char *__restrict__ ess,
                          const double *__restrict__ sign, const int *__restrict__ dof,
                          int eliminate, int maxrow, dcplx *__restrict__ vals) {
@@ -480,7 +514,7 @@ __global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__res
   const int p1 = ea_ptr[r + 1];
   for (int pp = ea_ptr[r]; pp < p1; ++pp) {
     const int id = ea[pp];
-    const dcplx *src = Ae + (size_t)id * nd;
+    const dcplx *src = Ae + (size_t)id * rs;
     const uint16_t *o = off + (size_t)pp * nd;
     double sa = 1.0;
     int ebase = 0;
