@@ -420,29 +420,38 @@ def run_e2e(a, case, dev, torch, stream) -> dict | None:
     out = torch.empty(2 * nnz, dtype=torch.float64, pin_memory=True)
     from lithofem_b200.asm import DeviceVector
     times = []
+    parts = []
     for it in range(1 + a.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g = AsmGpuGlobal(case.prob)
         assert g.Init(ad, dev)
+        t1 = time.perf_counter()
         assert g.BuildGlobal(ad.ess)
+        t2 = time.perf_counter()
         assert g.Assemble(True)
+        t3 = time.perf_counter()
         # D2H of the result (the CSR values) through a borrowed device view
         _, _, V, _, nz = g._csr()
         dv = torch.as_tensor(DeviceVector(V, (2 * nz,), "<f8"), device="cuda")
         out.copy_(dv)
         torch.cuda.synchronize()
         del dv
+        t4 = time.perf_counter()
         g.Release()
-        t1 = time.perf_counter()
+        t5 = time.perf_counter()
         if it >= 1:
-            times.append(t1 - t0)
+            times.append(t5 - t0)
+            parts.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4])
     t = float(np.median(times))
+    br = np.median(np.array(parts), axis=0) * 1e3
     return {"value": nnz / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(16 * nnz), "ms_per_step": 1e3 * t,
             "what": "lfasm_init (uploads from pinned host arrays) + lfasm_build_global "
                     "(device symbolic CSR + maps) + lfasm_assemble + D2H of the CSR values",
-            "timer": "host wall clock with device synchronize on both sides"}
+            "timer": "host wall clock with device synchronize on both sides",
+            "breakdown_ms": {"init": br[0], "build_global": br[1], "assemble": br[2],
+                             "d2h": br[3], "release": br[4]}}
 
 
 if __name__ == "__main__":

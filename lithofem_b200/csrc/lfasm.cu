@@ -120,6 +120,9 @@ struct lfasm_handle {
   // optional per-stage events of lfasm_assemble: prep+bulk, pml, gather
   int profile = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // side stream for the PML elements, overlapped with the bulk elements
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   // host copies of a caller-given symbolic CSR (read at init)
   std::vector<int> h_I, h_J;
 };
@@ -132,46 +135,66 @@ int sync_if(lfasm_handle *h) {
   return LFASM_OK;
 }
 
-// Element-independent tables of the bulk path: S_t[k][l] = quadrature sums
-// of reference shape products with the element's own rules (exact for the
-// polynomial integrands), symmetric pairs folded (j <= j').
+// Element-independent tables of the bulk path, quadrature sums of reference
+// shape products with the element's own rules (exact for these polynomial
+// integrands):  Scc_t[k][l] = sum_q w_q rc_k,a rc_l,b (+ the (b,a) term for
+// a != b), Svv_t likewise with vshapes, Rvc_jj'[k][l] = sum_q w_q rv_k,j rc_l,j'.
+// Packed per bulk-kernel thread (I, l >= 2I), value-major for coalesced
+// loads: [cc(2I,l) 6, vv(2I,l) 6, cc(2I+1,l) 6, vv(2I+1,l) 6,
+//         Rvc(2I,l) 9, Rvc(2I+1,l) 9, Rvc(l,2I) 9, Rvc(l,2I+1) 9].
+int bulk_threads(int ndp) { const int H = ndp / 2; return H * H + H; }
+
 void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
   const int nd = ad->nd;
-  S.assign((size_t)NT_ALL * ndp * ndp, 0.0);
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-  auto at = [&](int t, int k, int l) -> double & { return S[((size_t)t * ndp + k) * ndp + l]; };
   const lfasm_ref_rule &rc = ad->rule_cc, &rm = ad->rule_mass;
+  // full tables first: [9][nd][nd] each
+  std::vector<double> Rcc((size_t)9 * nd * nd, 0.0), Rvv(Rcc.size(), 0.0), Rvc(Rcc.size(), 0.0);
+  auto at = [&](std::vector<double> &T, int j, int k, int l) -> double & {
+    return T[((size_t)j * nd + k) * nd + l];
+  };
   for (int k = 0; k < nd; ++k)
     for (int l = 0; l < nd; ++l) {
-      double rcc[9] = {0}, rvv[9] = {0}, rvc[9] = {0}, rcv[9] = {0};
       for (int q = 0; q < rc.nq; ++q) {
         const double *ck = rc.curl + ((size_t)q * nd + k) * 3;
         const double *cl = rc.curl + ((size_t)q * nd + l) * 3;
-        const double w = rc.w[q];
         for (int j = 0; j < 3; ++j)
-          for (int jj = 0; jj < 3; ++jj) rcc[j * 3 + jj] += w * ck[j] * cl[jj];
+          for (int jj = 0; jj < 3; ++jj) at(Rcc, j * 3 + jj, k, l) += rc.w[q] * ck[j] * cl[jj];
       }
       for (int q = 0; q < rm.nq; ++q) {
         const double *vk = rm.vshape + ((size_t)q * nd + k) * 3;
         const double *vl = rm.vshape + ((size_t)q * nd + l) * 3;
-        const double *ck = rm.curl + ((size_t)q * nd + k) * 3;
         const double *cl = rm.curl + ((size_t)q * nd + l) * 3;
-        const double w = rm.w[q];
         for (int j = 0; j < 3; ++j)
           for (int jj = 0; jj < 3; ++jj) {
-            rvv[j * 3 + jj] += w * vk[j] * vl[jj];
-            rvc[j * 3 + jj] += w * vk[j] * cl[jj];
-            rcv[j * 3 + jj] += w * ck[j] * vl[jj];
+            at(Rvv, j * 3 + jj, k, l) += rm.w[q] * vk[j] * vl[jj];
+            at(Rvc, j * 3 + jj, k, l) += rm.w[q] * vk[j] * cl[jj];
           }
       }
-      for (int t = 0; t < 6; ++t) {
-        const int a = pa[t], b = pb[t];
-        at(t, k, l) = a == b ? rcc[a * 3 + a] : rcc[a * 3 + b] + rcc[b * 3 + a];
-        at(6 + t, k, l) = a == b ? rvv[a * 3 + a] : rvv[a * 3 + b] + rvv[b * 3 + a];
-      }
-      for (int t = 0; t < 9; ++t) {
-        at(12 + t, k, l) = rvc[t];
-        at(21 + t, k, l) = rcv[t];
+    }
+  auto sym = [&](std::vector<double> &T, int t, int k, int l) -> double {
+    if (k >= nd || l >= nd) return 0.0;
+    const int a = pa[t], b = pb[t];
+    return a == b ? at(T, a * 3 + a, k, l) : at(T, a * 3 + b, k, l) + at(T, b * 3 + a, k, l);
+  };
+  auto rvc = [&](int j, int k, int l) -> double {
+    return (k >= nd || l >= nd) ? 0.0 : at(Rvc, j, k, l);
+  };
+  const int nthr = bulk_threads(ndp);
+  S.assign((size_t)60 * nthr, 0.0);
+  int f = 0;
+  for (int I = 0; I < ndp / 2; ++I)
+    for (int l = 2 * I; l < ndp; ++l, ++f) {
+      for (int a = 0; a < 2; ++a) {
+        const int r = 2 * I + a;
+        for (int t = 0; t < 6; ++t) {
+          S[(size_t)(12 * a + t) * nthr + f] = sym(Rcc, t, r, l);
+          S[(size_t)(12 * a + 6 + t) * nthr + f] = sym(Rvv, t, r, l);
+        }
+        for (int j = 0; j < 9; ++j) {
+          S[(size_t)(24 + 9 * a + j) * nthr + f] = rvc(j, r, l);
+          S[(size_t)(42 + 9 * a + j) * nthr + f] = rvc(j, l, r);
+        }
       }
     }
 }
@@ -428,6 +451,9 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   // sector and column pairs fill whole sectors
   LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * h->ndp * sizeof(dcplx)));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
+  LF_CUDA_H(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  LF_CUDA_H(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+  LF_CUDA_H(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming));
   LF_CUDA_H(cudaDeviceSynchronize());
 #undef LF_CUDA_H
   *out = h;
@@ -457,15 +483,15 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
 
 template <int NDP8>
 static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int mask_mass, int te,
-                      int eliminate, int rs) {
+                      int eliminate, int rs, cudaStream_t st) {
   const size_t smem = PmlShape<NDP8>::SMEM;
-  const int threads = NDP8 * 4;
+  const int threads = NDP8 * PML_QC;
   auto go = [&](auto kern) -> int {
     LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     LF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
     const int grid = std::max(1, std::min(h->n_pml, std::max(per_sm, 1) * h->sm_count));
-    kern<<<grid, threads, smem, h->stream>>>(
+    kern<<<grid, threads, smem, st>>>(
         h->n_pml, h->pml_list, h->nd, rs, h->p, h->rcc.view(), h->rm.view(), h->J, h->Jinv,
         h->detJ, h->v0, h->attr, h->eps_tab, h->elem_eps, h->pml, mask_cc, mask_mass, te,
         eliminate, h->fopack, h->signmask, h->essmask, h->Ae);
@@ -487,8 +513,16 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
   const int mask = mask_cc | mask_mass;
   const bool cross = (mask & (LFASM_CROSS0 | LFASM_CROSS1)) != 0;
   const bool prof = mode == 1 && h->profile;
-  // every element is written by exactly one of the two paths: no memset
+  // every element is written by exactly one of the two paths: no memset.
+  // The PML elements (tensor-pipe bound) run on the side stream next to the
+  // bulk elements (HBM bound) unless stage timing is requested.
+  const bool overlap = !prof && h->n_bulk > 0 && h->n_pml > 0;
+  cudaStream_t pst = overlap ? h->side : h->stream;
   if (prof) LF_CUDA(cudaEventRecord(h->ev[0], h->stream));
+  if (overlap) {
+    LF_CUDA(cudaEventRecord(h->fork, h->stream));
+    LF_CUDA(cudaStreamWaitEvent(h->side, h->fork, 0));
+  }
   const int rs = mode ? h->ndp : h->nd;
   if (h->n_bulk) {
     const int nb = h->n_bulk;
@@ -496,16 +530,19 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
                                                          h->detJ, h->attr, h->eps_tab,
                                                          h->elem_eps, h->pml, mask, h->rec);
     LF_LAUNCHED();
-    const int ytiles = ((h->ndp / 2) * h->ndp + BULK_THREADS - 1) / BULK_THREADS;
+    const int nthr = bulk_threads(h->ndp);
+    const int ytiles = (nthr + BULK_THREADS - 1) / BULK_THREADS;
     // about two waves of resident blocks; each block keeps its S-table
     // values in registers across its chunk of elements
     const long long want = (long long)h->sm_count * 8;
     int chunk = (int)std::max<long long>(16, ((long long)nb * ytiles + want - 1) / want);
+    chunk = (chunk + BULK_EB - 1) / BULK_EB * BULK_EB;
     dim3 grid((nb + chunk - 1) / chunk, ytiles);
 #define LF_BULK(C, M)                                                             \
   k_bulk<C, M><<<grid, BULK_THREADS, 0, h->stream>>>(                             \
-      nb, h->bulk_list, h->rec, h->S, h->nd, h->ndp, h->p, chunk, te, eliminate,  \
-      rs, h->fopack, h->signmask, h->essmask, h->Ae)
+      nb, h->bulk_list, h->rec, h->S, nthr, h->nd, h->ndp, h->p, chunk, te,       \
+      eliminate, rs, (mask & LFASM_CROSS0) ? 1 : 0, (mask & LFASM_CROSS1) ? 1 : 0,  \
+      h->fopack, h->signmask, h->essmask, h->Ae)
     if (cross) { if (mode) LF_BULK(true, 1); else LF_BULK(true, 0); }
     else { if (mode) LF_BULK(false, 1); else LF_BULK(false, 0); }
 #undef LF_BULK
@@ -513,10 +550,14 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[1], h->stream));
   if (h->n_pml) {
-    int rc = h->p == 1 ? launch_pml<8>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs)
-           : h->p == 2 ? launch_pml<24>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs)
-                       : launch_pml<48>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs);
+    int rc = h->p == 1 ? launch_pml<8>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
+           : h->p == 2 ? launch_pml<24>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
+                       : launch_pml<48>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst);
     if (rc) return rc;
+  }
+  if (overlap) {
+    LF_CUDA(cudaEventRecord(h->join, h->side));
+    LF_CUDA(cudaStreamWaitEvent(h->stream, h->join, 0));
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[2], h->stream));
   return LFASM_OK;
@@ -897,6 +938,9 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->red);
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->side) cudaStreamDestroy(h->side);
   delete h;
 }
 
