@@ -37,7 +37,6 @@ struct Rule {
   const double *ip, *w, *v, *c;
 };
 
-constexpr int REC = 28;        // doubles per bulk-element coefficient record
 constexpr int NT_CC = 6;       // symmetric (j <= j') pairs
 constexpr int NT_ALL = 30;     // 6 cc + 6 vv + 9 vc + 9 cv
 constexpr int BULK_THREADS = 128;
@@ -66,6 +65,12 @@ __device__ __forceinline__ dcplx pml_s(const PmlParams &p, double z) {
   return mk(1.0, smax * pow(d, p.order));
 }
 
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ int face_of(int k, int p) {
   const int f0 = 6 * p, nf = p * (p - 1);
   if (nf == 0 || k < f0 || k >= f0 + 4 * nf) return -1;
@@ -73,14 +78,26 @@ __device__ __forceinline__ int face_of(int k, int p) {
 }
 
 // ---------------------------------------------------------------------------
-// bulk-element coefficient records (REC doubles per element)
-//   [0,6)   gcc: J^T J / detJ at the symmetric pairs (00,11,22,01,02,12)
-//   [6,18)  gvv: detJ Jinv (-k0^2 eps I - K K) Jinv^T, complex, same pairs
-//   [18,27) gx : Jinv K J (the cross coefficients, i factored out), j*3+j'
-// With these, A = Sym + i (c0 X - c1 X^T): Sym = sum gcc Scc + gvv Svv is
-// symmetric and X = sum gx Rvc; the MixedVectorWeakCurl coefficient is
-// J^T K Jinv^T = -(Jinv K J)^T, which turns its term into -X^T.
+// Bulk elements as a tensor-core GEMM.
+//
+// For an element with s == 1 at every quadrature point the element matrix is
+//   A_e = sum_t G_e[t] S_t,   t over 32 terms (30 used):
+//   t  0.. 5  curl-curl, symmetric pairs (00,11,22,01,02,12): G = J^T J / detJ
+//   t  6..11  mass + KLK, same pairs: G = detJ Jinv (-k0^2 eps I - K K) Jinv^T
+//   t 12..20  MixedVectorCurl (j*3+j'):      G = i Jinv K J
+//   t 21..29  MixedVectorWeakCurl (j*3+j'):  G = i J^T K Jinv^T
+// with S_t the element-independent reference quadrature sums.  Written as
+// C (8 elements x 8 entries) = A (8 x 32) B (32 x 8) per m8n8k4 DMMA tile:
+// A = the element coefficient rows (a real row: t 0..11, an imaginary row:
+// t 6..29), B = S in "pair-block-major" entry order n = 4 pb + 2a + b for the
+// 2x2 pair block pb = (I, J) and entry (2I+a, 2J+b).  Each warp keeps the B
+// fragments of its N tiles in registers for the whole kernel.
 // ---------------------------------------------------------------------------
+constexpr int BK = 32;          // coefficient terms (padded)
+constexpr int BREC = 2 * BK;    // doubles per element record: real row, imaginary row
+constexpr int BULK_T = 4;       // N tiles (8 entries) per warp
+constexpr int BULK_WARPS = 4;
+
 __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
                             const double *__restrict__ J9, const double *__restrict__ Ji9,
                             const double *__restrict__ detJ, const int *__restrict__ attr,
@@ -98,9 +115,9 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
   }
   const double det = detJ[e];
   const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
-  double *r = rec + (size_t)i * REC;
+  double *re = rec + (size_t)i * BREC, *im = re + BK;
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-  const bool cc = mask & 1, ms = mask & 2, kl = mask & 16;
+  const bool cc = mask & 1, ms = mask & 2, c0 = mask & 4, c1 = mask & 8, kl = mask & 16;
   const double kx = pml.kx, ky = pml.ky, k2 = pml.k0 * pml.k0;
   // K = [[0,0,ky],[0,0,-kx],[-ky,kx,0]] (fill_K, problem_common.inc:150-158)
   const double K[9] = {0.0, 0.0, ky, 0.0, 0.0, -kx, -ky, kx, 0.0};
@@ -108,11 +125,10 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
   const double mKK[9] = {ky * ky, -kx * ky, 0.0, -kx * ky, kx * kx, 0.0, 0.0, 0.0,
                          kx * kx + ky * ky};
   const double me_re = -k2 * eps.re, me_im = -k2 * eps.im;
+  for (int t = 0; t < BK; ++t) { re[t] = 0.0; im[t] = 0.0; }
   for (int t = 0; t < 6; ++t) {
     const int a = pa[t], b = pb[t];
-    double g = 0.0;
-    if (cc) g = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
-    r[t] = g;
+    if (cc) re[t] = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
     const double jj = Ji[a * 3 + 0] * Ji[b * 3 + 0] + Ji[a * 3 + 1] * Ji[b * 3 + 1] +
                       Ji[a * 3 + 2] * Ji[b * 3 + 2];
     double vr = 0.0, vi = 0.0;
@@ -123,161 +139,129 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
         for (int c2 = 0; c2 < 3; ++c2) s += Ji[a * 3 + rr] * mKK[rr * 3 + c2] * Ji[b * 3 + c2];
       vr += s;
     }
-    r[6 + 2 * t] = det * vr;
-    r[7 + 2 * t] = det * vi;
+    re[6 + t] = det * vr;
+    im[6 + t] = det * vi;
   }
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
-      double gx = 0.0;
+      double gvc = 0.0, gcv = 0.0;
       for (int rr = 0; rr < 3; ++rr)
         for (int c2 = 0; c2 < 3; ++c2) {
           const double k = K[rr * 3 + c2];
-          if (k != 0.0) gx += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
+          if (k == 0.0) continue;
+          gvc += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
+          gcv += J[rr * 3 + a] * k * Ji[b * 3 + c2];
         }
-      r[18 + a * 3 + b] = gx;
+      if (c0) im[12 + a * 3 + b] = gvc;
+      if (c1) im[21 + a * 3 + b] = gcv;
     }
-  r[27] = 0.0;
 }
 
-// ---------------------------------------------------------------------------
-// bulk element kernel.  Thread <-> (row pair I, column l >= 2I): it produces
-// A(2I+a, l) and, when l >= 2I+2, the mirrored A(l, 2I+a), a = 0, 1, from NV
-// table values held in registers (symmetric tables at (2I+a, l), cross
-// tables at (2I+a, l) and (l, 2I+a)).  Element records are staged through
-// shared memory in batches of BULK_EB.  Face transforms: the row pair is
-// thread-local, the partner column / row l^1 sits in the neighbouring lane.
-// MODE 0: raw local matrix (ComputeLocal); MODE 1: signs + elimination.
-// ---------------------------------------------------------------------------
-constexpr int BULK_EB = 8;
-
+// ncol_tiles: total N tiles (entries / 8, rounded up); nbatch: element batches
+// of 8.  Block: BULK_WARPS warps, N tiles [blockIdx.y*BULK_WARPS*BULK_T, ...).
 template <bool CROSS, int MODE>
-__global__ void __launch_bounds__(BULK_THREADS)
+__global__ void __launch_bounds__(BULK_WARPS * 32)
 k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
-       const double *__restrict__ S, int nthr, int nd, int ndp, int p, int chunk, int te,
-       int eliminate, int rs, int c0, int c1, const unsigned *__restrict__ fopack,
+       const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
+       int eliminate, int rs, const unsigned *__restrict__ fopack,
        const unsigned long long *__restrict__ signmask,
        const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
-  constexpr int NV = CROSS ? 60 : 24;
-  __shared__ double sg[BULK_EB * REC];
-  __shared__ int se[BULK_EB];
-  const int tid = threadIdx.x;
-  const int f = blockIdx.y * BULK_THREADS + tid;
-  const bool valid = f < nthr;
-  int I = 0, l = 0;
-  if (valid) {
-    int rem = f;
-    while (rem >= ndp - 2 * I) { rem -= ndp - 2 * I; ++I; }
-    l = 2 * I + rem;
+  __shared__ double sA[8 * BREC];
+  __shared__ int se[8];
+  __shared__ unsigned sfo[8];
+  __shared__ unsigned long long ssm[8], sem[8];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int H = ndp >> 1, npb = H * H;
+  // B fragments: b[T][k-step] = S[kstep*4 + t4][tile*8 + g]
+  constexpr int KS = BK / 4;
+  double bf[BULK_T][KS];
+  int tile0 = (blockIdx.y * BULK_WARPS + w) * BULK_T;
+#pragma unroll
+  for (int j = 0; j < BULK_T; ++j) {
+    const int tile = tile0 + j;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks)
+      bf[j][ks] = tile < ntiles ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
   }
-  const bool mirror = valid && l >= 2 * I + 2;
-  const int r0 = 2 * I, r1 = 2 * I + 1;
-  double sv[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) sv[v] = valid ? S[(size_t)v * nthr + f] : 0.0;
-  const int frow = valid ? face_of(r0, p) : -1;
-  const int fcol = valid ? face_of(l & ~1, p) : -1;
-  const int cp = l & 1;
-  const double fc0 = c0 ? 1.0 : 0.0, fc1 = c1 ? 1.0 : 0.0;
-  const int i0 = blockIdx.x * chunk;
-  const int i1 = min(nb, i0 + chunk);
-  for (int ib = i0; ib < i1; ib += BULK_EB) {
-    const int nbat = min(BULK_EB, i1 - ib);
+  // entries owned in the epilogue: n = tile*8 + 2*t4 + {0,1} -> pair block
+  // pb = tile*2 + (t4 >> 1), row half a = t4 & 1, columns 2J, 2J+1
+  const int nbat = (nb + 7) / 8;
+  const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
+  for (int bt = b0; bt < b1; ++bt) {
+    const int ebase = bt * 8;
+    const int nel = min(8, nb - ebase);
     __syncthreads();
-    for (int j = tid; j < nbat * REC; j += BULK_THREADS) sg[j] = rec[(size_t)ib * REC + j];
-    if (tid < nbat) se[tid] = list[ib + tid];
-    __syncthreads();
-    for (int b = 0; b < nbat; ++b) {
-      const double *g = sg + b * REC;
-      double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
-#pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        const double gc = g[t];
-        sr0 = fma(gc, sv[t], sr0);
-        sr1 = fma(gc, sv[12 + t], sr1);
-      }
-#pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        const double gr = g[6 + 2 * t], gi = g[7 + 2 * t];
-        sr0 = fma(gr, sv[6 + t], sr0);
-        si0 = fma(gi, sv[6 + t], si0);
-        sr1 = fma(gr, sv[18 + t], sr1);
-        si1 = fma(gi, sv[18 + t], si1);
-      }
-      // primary A(r0|r1, l) and mirror A(l, r0|r1)
-      double pr0 = sr0, pi0 = si0, pr1 = sr1, pi1 = si1;
-      double mr0 = sr0, mi0 = si0, mr1 = sr1, mi1 = si1;
-      if (CROSS) {
-        double x0 = 0.0, x1 = 0.0, y0 = 0.0, y1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-          const double gx = g[18 + t];
-          x0 = fma(gx, sv[(24 + t) % NV], x0);
-          x1 = fma(gx, sv[(33 + t) % NV], x1);
-          y0 = fma(gx, sv[(42 + t) % NV], y0);
-          y1 = fma(gx, sv[(51 + t) % NV], y1);
+    for (int j = tid; j < 8 * BREC; j += BULK_WARPS * 32)
+      sA[j] = (j / BREC) < nel ? rec[(size_t)ebase * BREC + j] : 0.0;
+    if (tid < 8) {
+      const int e = tid < nel ? list[ebase + tid] : -1;
+      se[tid] = e;
+      if (e >= 0) {
+        sfo[tid] = fopack[e];
+        if (MODE == 1) {
+          ssm[tid] = signmask[e];
+          sem[tid] = eliminate ? essmask[e] : 0ull;
         }
-        pi0 += fc0 * x0 - fc1 * y0;
-        pi1 += fc0 * x1 - fc1 * y1;
-        mi0 += fc0 * y0 - fc1 * x0;
-        mi1 += fc0 * y1 - fc1 * x1;
       }
-      const int e = se[b];
+    }
+    __syncthreads();
+    // A fragments: A[g][kstep*4 + t4] (real row) and imaginary row
+    double ar[3], ai[KS];
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * BREC + ks * 4 + t4];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) ai[ks] = sA[g * BREC + BK + ks * 4 + t4];
+    const int e = se[g];
+#pragma unroll
+    for (int j = 0; j < BULK_T; ++j) {
+      double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 3; ++ks) dmma(cr0, cr1, ar[ks], bf[j][ks]);
+#pragma unroll
+      for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci0, ci1, ai[ks], bf[j][ks]);
+      const int tile = tile0 + j;
+      const int pb = tile * 2 + (t4 >> 1);
+      const int a = t4 & 1;
+      const bool ok = tile < ntiles && pb < npb && e >= 0;
+      const int I = ok ? pb / H : 0, Jp = ok ? pb - I * H : 0;
+      const int row = 2 * I + a, col = 2 * Jp;
+      // dual transform: columns (local pair), rows (partner lane t4^1)
       if (te && p >= 2) {
-        const unsigned fp = fopack[e];
-        // primary: columns (partner lane holds column l^1), then rows
-        const double qpr0 = __shfl_xor_sync(0xffffffffu, pr0, 1);
-        const double qpi0 = __shfl_xor_sync(0xffffffffu, pi0, 1);
-        const double qpr1 = __shfl_xor_sync(0xffffffffu, pr1, 1);
-        const double qpi1 = __shfl_xor_sync(0xffffffffu, pi1, 1);
-        // mirror: rows l / l^1 across the lane pair, columns local
-        const double qmr0 = __shfl_xor_sync(0xffffffffu, mr0, 1);
-        const double qmi0 = __shfl_xor_sync(0xffffffffu, mi0, 1);
-        const double qmr1 = __shfl_xor_sync(0xffffffffu, mr1, 1);
-        const double qmi1 = __shfl_xor_sync(0xffffffffu, mi1, 1);
-        if (fcol >= 0) {
-          const double *T = c_tinv + 4 * ((fp >> (8 * fcol)) & 0xffu);
-          // M[c'][c] = T[2c + c']: new[cp] = own * T[2cp+cp] + other * T[2cp+1-cp]
-          const double own = T[2 * cp + cp], oth = T[2 * cp + 1 - cp];
-          double n0 = own * pr0 + oth * qpr0, n1 = own * pi0 + oth * qpi0;
-          double n2 = own * pr1 + oth * qpr1, n3 = own * pi1 + oth * qpi1;
-          pr0 = n0; pi0 = n1; pr1 = n2; pi1 = n3;
-          n0 = own * mr0 + oth * qmr0; n1 = own * mi0 + oth * qmi0;
-          n2 = own * mr1 + oth * qmr1; n3 = own * mi1 + oth * qmi1;
-          mr0 = n0; mi0 = n1; mr1 = n2; mi1 = n3;
+        const unsigned fp = sfo[g];
+        const int fc = face_of(col, p);
+        if (ok && fc >= 0) {
+          const double *T = c_tinv + 4 * ((fp >> (8 * fc)) & 0xffu);
+          const double n0 = T[0] * cr0 + T[1] * cr1, n1 = T[2] * cr0 + T[3] * cr1;
+          const double m0 = T[0] * ci0 + T[1] * ci1, m1 = T[2] * ci0 + T[3] * ci1;
+          cr0 = n0; cr1 = n1; ci0 = m0; ci1 = m1;
         }
-        if (frow >= 0) {
-          const double *T = c_tinv + 4 * ((fp >> (8 * frow)) & 0xffu);
-          double n0 = T[0] * pr0 + T[1] * pr1, n1 = T[0] * pi0 + T[1] * pi1;
-          double n2 = T[2] * pr0 + T[3] * pr1, n3 = T[2] * pi0 + T[3] * pi1;
-          pr0 = n0; pi0 = n1; pr1 = n2; pi1 = n3;
-          n0 = T[0] * mr0 + T[1] * mr1; n1 = T[0] * mi0 + T[1] * mi1;
-          n2 = T[2] * mr0 + T[3] * mr1; n3 = T[2] * mi0 + T[3] * mi1;
-          mr0 = n0; mi0 = n1; mr1 = n2; mi1 = n3;
+        const double qr0 = __shfl_xor_sync(0xffffffffu, cr0, 1);
+        const double qr1 = __shfl_xor_sync(0xffffffffu, cr1, 1);
+        const double qi0 = __shfl_xor_sync(0xffffffffu, ci0, 1);
+        const double qi1 = __shfl_xor_sync(0xffffffffu, ci1, 1);
+        const int fr = face_of(2 * I, p);
+        if (ok && fr >= 0) {
+          const double *T = c_tinv + 4 * ((fp >> (8 * fr)) & 0xffu);
+          const double own = T[2 * a + a], oth = T[2 * a + 1 - a];
+          cr0 = own * cr0 + oth * qr0; cr1 = own * cr1 + oth * qr1;
+          ci0 = own * ci0 + oth * qi0; ci1 = own * ci1 + oth * qi1;
         }
       }
-      if (MODE == 1 && valid) {
-        const unsigned long long sm = signmask[e];
-        const double sl = ((sm >> l) & 1ull) ? -1.0 : 1.0;
-        const double sa = (((sm >> r0) & 1ull) ? -1.0 : 1.0) * sl;
-        const double sb = (((sm >> r1) & 1ull) ? -1.0 : 1.0) * sl;
-        pr0 *= sa; pi0 *= sa; pr1 *= sb; pi1 *= sb;
-        mr0 *= sa; mi0 *= sa; mr1 *= sb; mi1 *= sb;
-        if (eliminate) {
-          const unsigned long long em = essmask[e];
-          const bool el = (em >> l) & 1ull;
-          if (el || ((em >> r0) & 1ull)) { pr0 = pi0 = mr0 = mi0 = 0.0; }
-          if (el || ((em >> r1) & 1ull)) { pr1 = pi1 = mr1 = mi1 = 0.0; }
-        }
+      if (!ok || row >= nd || col >= nd) continue;
+      if (MODE == 1) {
+        const unsigned long long sm = ssm[g], em = sem[g];
+        const double sr = ((sm >> row) & 1ull) ? -1.0 : 1.0;
+        const double s0 = sr * (((sm >> col) & 1ull) ? -1.0 : 1.0);
+        const double s1 = sr * (((sm >> (col + 1)) & 1ull) ? -1.0 : 1.0);
+        cr0 *= s0; ci0 *= s0; cr1 *= s1; ci1 *= s1;
+        const bool er = (em >> row) & 1ull;
+        if (er || ((em >> col) & 1ull)) { cr0 = 0.0; ci0 = 0.0; }
+        if (er || ((em >> (col + 1)) & 1ull)) { cr1 = 0.0; ci1 = 0.0; }
       }
-      if (valid && l < nd) {
-        dcplx *dst = Ae + (size_t)e * nd * rs;
-        dst[(size_t)r0 * rs + l] = mk(pr0, pi0);
-        if (r1 < nd) dst[(size_t)r1 * rs + l] = mk(pr1, pi1);
-        if (mirror) {
-          dst[(size_t)l * rs + r0] = mk(mr0, mi0);
-          if (r1 < nd) dst[(size_t)l * rs + r1] = mk(mr1, mi1);
-        }
-      }
+      dcplx *dst = Ae + (size_t)e * nd * rs + (size_t)row * rs + col;
+      dst[0] = mk(cr0, ci0);
+      if (col + 1 < nd) dst[1] = mk(cr1, ci1);
     }
   }
 }
@@ -294,7 +278,7 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 // M tiles, so the epilogue holds both parts of each entry.  Rows are staged
 // in chunks of PML_QC points; blocks are persistent over the PML elements.
 // ---------------------------------------------------------------------------
-constexpr int PML_QC = 4;  // quadrature points per staged chunk (blockDim = PML_QC * NDP8)
+constexpr int PML_QMAX = 8;  // max quadrature points per staged chunk (blockDim = QC * NDP8)
 
 struct QCoef {  // per quadrature point, already multiplied by w_q detJ
   dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries (cc rule: Lambda^-1 diagonal)
@@ -302,20 +286,18 @@ struct QCoef {  // per quadrature point, already multiplied by w_q detJ
   dcplx c02, c12, c20, c21;           // M1 = i Lambda^-1 K
 };
 
-__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
-template <int NDP8>
+template <int NDP8, int QC>
 struct PmlShape {
-  static constexpr int NW = NDP8 / 8;                    // warps = column tiles
+  static constexpr int NW = NDP8 / 8;                    // column tiles
   static constexpr int MT = NDP8 / 8;                    // row tiles
+  static constexpr int WPC = QC / 4;                     // warps per column tile
+  static constexpr int MTW = MT / WPC;                   // row tiles per warp
+  static_assert(MT % WPC == 0, "row tiles must split evenly");
+  static constexpr int THREADS = QC * NDP8;
   static constexpr int LD = (NDP8 % 16 == 0) ? NDP8 + 8 : NDP8;  // row stride = 8 mod 16
-  static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
+  static constexpr int RMAX = QC * 6;                    // rows per chunk (multiple of 4)
   static constexpr int BUF = 3 * RMAX * LD;              // X, Yre, Yim of one chunk
-  static constexpr size_t SMEM = (size_t)2 * BUF * sizeof(double) + 2 * PML_QC * sizeof(QCoef);
+  static constexpr size_t SMEM = (size_t)2 * BUF * sizeof(double) + 2 * QC * sizeof(QCoef);
 };
 
 __device__ __forceinline__ void pml_coef(QCoef &c, int rule, int mask, const Rule &R, int q,
@@ -360,8 +342,8 @@ __device__ __forceinline__ void pml_coef(QCoef &c, int rule, int mask, const Rul
   } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
 }
 
-template <int NDP8, bool CROSS, int MODE>
-__global__ void __launch_bounds__(NDP8 * PML_QC)
+template <int NDP8, int QC, bool CROSS, int MODE>
+__global__ void __launch_bounds__(NDP8 * QC)
 k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
           const double *__restrict__ J9, const double *__restrict__ Ji9,
           const double *__restrict__ detJ, const double *__restrict__ v0,
@@ -370,16 +352,19 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
           int te, int eliminate, const unsigned *__restrict__ fopack,
           const unsigned long long *__restrict__ signmask,
           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
-  using Sh = PmlShape<NDP8>;
-  constexpr int LD = Sh::LD, MT = Sh::MT, RMAX = Sh::RMAX, BUF = Sh::BUF;
+  using Sh = PmlShape<NDP8, QC>;
+  constexpr int LD = Sh::LD, RMAX = Sh::RMAX, BUF = Sh::BUF, NW = Sh::NW, MTW = Sh::MTW;
+  constexpr int PML_QC = QC;
   extern __shared__ double smem[];
   QCoef *qcb = reinterpret_cast<QCoef *>(smem + 2 * BUF);  // [2][PML_QC]
   __shared__ double sJ[9], sJi[9], sdet, sv0z;
   __shared__ dcplx seps;
   __shared__ unsigned sfo;
 
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
+  const int w = wid % NW;               // column tile of this warp
+  const int mbase = (wid / NW) * MTW;   // first row tile of this warp
   // staging item of this thread: quadrature point qi of the chunk, column k
   const int qi = tid / NDP8, k = tid - qi * NDP8;
   const bool cross_on = CROSS && (mask_mass & (4 | 8));
@@ -490,9 +475,9 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
       seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
       sfo = fopack[e];
     }
-    double cr[MT][2], ci[MT][2];
+    double cr[MTW][2], ci[MTW][2];
 #pragma unroll
-    for (int m = 0; m < MT; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
+    for (int m = 0; m < MTW; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
     __syncthreads();
     coefs(0);
     __syncthreads();
@@ -510,8 +495,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
         const double br = Yr[(r0 + t4) * LD + w * 8 + g];
         const double bi = Yi[(r0 + t4) * LD + w * 8 + g];
 #pragma unroll
-        for (int m = 0; m < MT; ++m) {
-          const double a = Xs[(r0 + t4) * LD + m * 8 + g];
+        for (int m = 0; m < MTW; ++m) {
+          const double a = Xs[(r0 + t4) * LD + (mbase + m) * 8 + g];
           dmma(cr[m][0], cr[m][1], a, br);
           dmma(ci[m][0], ci[m][1], a, bi);
         }
@@ -524,8 +509,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
     dcplx *dst = Ae + (size_t)e * nd * rs;
     const int col = w * 8 + 2 * t4;
 #pragma unroll
-    for (int m = 0; m < MT; ++m) {
-      const int row = m * 8 + g;
+    for (int m = 0; m < MTW; ++m) {
+      const int row = (mbase + m) * 8 + g;
       if (row >= nd) continue;
       dcplx v2[2];
 #pragma unroll
@@ -571,37 +556,7 @@ __global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__res
   __syncwarp();
   const bool row_ess = eliminate && ess[r];
   const int p1 = ea_ptr[r + 1];
-  if (!RAW && nd <= 64) {
-    // prefetch GATHER_U element rows (2 lane-halves each) before the ordered
-    // accumulation: more loads in flight, same summation order
-    constexpr int U = 4;
-    for (int pp = ea_ptr[r]; pp < p1; pp += U) {
-      dcplx v[U][2];
-      int jo[U][2];
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-          const int b = lane + 32 * hh;
-          jo[u][hh] = -1;
-          if (pp + u < p1 && b < nd) {
-            const int id = ea[pp + u];
-            v[u][hh] = Ae[(size_t)id * rs + b];
-            jo[u][hh] = off[(size_t)(pp + u) * nd + b];
-          }
-        }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh)
-          if (jo[u][hh] >= 0) {
-            acc[jo[u][hh]].re += v[u][hh].re;
-            acc[jo[u][hh]].im += v[u][hh].im;
-          }
-        __syncwarp();
-      }
-    }
-  } else {
+  {
     for (int pp = ea_ptr[r]; pp < p1; ++pp) {
       const int id = ea[pp];
       const dcplx *src = Ae + (size_t)id * rs;
