@@ -135,22 +135,21 @@ int sync_if(lfasm_handle *h) {
   return LFASM_OK;
 }
 
-// Element-independent B operand of the bulk GEMM: quadrature sums of
-// reference shape products with the element's own rules (exact for these
-// polynomial integrands), term-major [BK][ntiles*8], entries in pair-block
-// order n = 4 (I*H + J) + 2a + b for entry (2I+a, 2J+b), H = ndp/2:
-//   t 0..5   Scc: sum_q w rc_k,a rc_l,b (+ (b,a) term) at the symmetric pairs
-//   t 6..11  Svv: same with vshapes (rule_mass)
-//   t 12..20 Rvc_jj' = sum_q w rv_k,j rc_l,j'
-//   t 21..29 Rcv_jj' = sum_q w rc_k,j rv_l,j'
-int bulk_tiles(int ndp) { const int H = ndp / 2; return (4 * H * H + 7) / 8; }
+// Element-independent tables of the bulk path, quadrature sums of reference
+// shape products with the element's own rules (exact for these polynomial
+// integrands):  Scc_t[k][l] = sum_q w_q rc_k,a rc_l,b (+ the (b,a) term for
+// a != b), Svv_t likewise with vshapes, Rvc_jj'[k][l] = sum_q w_q rv_k,j rc_l,j'.
+// Packed per bulk-kernel thread (I, l >= 2I), value-major for coalesced
+// loads: [cc(2I,l) 6, vv(2I,l) 6, cc(2I+1,l) 6, vv(2I+1,l) 6,
+//         Rvc(2I,l) 9, Rvc(2I+1,l) 9, Rvc(l,2I) 9, Rvc(l,2I+1) 9].
+int bulk_threads(int ndp) { const int H = ndp / 2; return H * H + H; }
 
 void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
   const int nd = ad->nd;
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
   const lfasm_ref_rule &rc = ad->rule_cc, &rm = ad->rule_mass;
-  std::vector<double> Rcc((size_t)9 * nd * nd, 0.0), Rvv(Rcc.size(), 0.0), Rvc(Rcc.size(), 0.0),
-      Rcv(Rcc.size(), 0.0);
+  // full tables first: [9][nd][nd] each
+  std::vector<double> Rcc((size_t)9 * nd * nd, 0.0), Rvv(Rcc.size(), 0.0), Rvc(Rcc.size(), 0.0);
   auto at = [&](std::vector<double> &T, int j, int k, int l) -> double & {
     return T[((size_t)j * nd + k) * nd + l];
   };
@@ -165,37 +164,39 @@ void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
       for (int q = 0; q < rm.nq; ++q) {
         const double *vk = rm.vshape + ((size_t)q * nd + k) * 3;
         const double *vl = rm.vshape + ((size_t)q * nd + l) * 3;
-        const double *ck = rm.curl + ((size_t)q * nd + k) * 3;
         const double *cl = rm.curl + ((size_t)q * nd + l) * 3;
         for (int j = 0; j < 3; ++j)
           for (int jj = 0; jj < 3; ++jj) {
             at(Rvv, j * 3 + jj, k, l) += rm.w[q] * vk[j] * vl[jj];
             at(Rvc, j * 3 + jj, k, l) += rm.w[q] * vk[j] * cl[jj];
-            at(Rcv, j * 3 + jj, k, l) += rm.w[q] * ck[j] * vl[jj];
           }
       }
     }
-  const int H = ndp / 2, ntiles = bulk_tiles(ndp), N = ntiles * 8;
-  S.assign((size_t)BK * N, 0.0);
-  for (int I = 0; I < H; ++I)
-    for (int Jp = 0; Jp < H; ++Jp)
-      for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b) {
-          const int k = 2 * I + a, l = 2 * Jp + b;
-          if (k >= nd || l >= nd) continue;
-          const size_t n = (size_t)4 * (I * H + Jp) + 2 * a + b;
-          for (int t = 0; t < 6; ++t) {
-            const int x = pa[t], y = pb[t];
-            S[(size_t)t * N + n] = x == y ? at(Rcc, x * 3 + x, k, l)
-                                          : at(Rcc, x * 3 + y, k, l) + at(Rcc, y * 3 + x, k, l);
-            S[(size_t)(6 + t) * N + n] = x == y ? at(Rvv, x * 3 + x, k, l)
-                                                : at(Rvv, x * 3 + y, k, l) + at(Rvv, y * 3 + x, k, l);
-          }
-          for (int j = 0; j < 9; ++j) {
-            S[(size_t)(12 + j) * N + n] = at(Rvc, j, k, l);
-            S[(size_t)(21 + j) * N + n] = at(Rcv, j, k, l);
-          }
+  auto sym = [&](std::vector<double> &T, int t, int k, int l) -> double {
+    if (k >= nd || l >= nd) return 0.0;
+    const int a = pa[t], b = pb[t];
+    return a == b ? at(T, a * 3 + a, k, l) : at(T, a * 3 + b, k, l) + at(T, b * 3 + a, k, l);
+  };
+  auto rvc = [&](int j, int k, int l) -> double {
+    return (k >= nd || l >= nd) ? 0.0 : at(Rvc, j, k, l);
+  };
+  const int nthr = bulk_threads(ndp);
+  S.assign((size_t)60 * nthr, 0.0);
+  int f = 0;
+  for (int I = 0; I < ndp / 2; ++I)
+    for (int l = 2 * I; l < ndp; ++l, ++f) {
+      for (int a = 0; a < 2; ++a) {
+        const int r = 2 * I + a;
+        for (int t = 0; t < 6; ++t) {
+          S[(size_t)(12 * a + t) * nthr + f] = sym(Rcc, t, r, l);
+          S[(size_t)(12 * a + 6 + t) * nthr + f] = sym(Rvv, t, r, l);
         }
+        for (int j = 0; j < 9; ++j) {
+          S[(size_t)(24 + 9 * a + j) * nthr + f] = rvc(j, r, l);
+          S[(size_t)(42 + 9 * a + j) * nthr + f] = rvc(j, l, r);
+        }
+      }
+    }
 }
 
 // 2x2 blocks relating element-local face DOF pairs to the global pairs for
@@ -397,7 +398,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   h->n_pml = (int)pl.size();
   LF_CUDA_H(upload(h->bulk_list, bl.data(), bl.size()));
   LF_CUDA_H(upload(h->pml_list, pl.data(), pl.size()));
-  if (h->n_bulk) LF_CUDA_H(cudaMalloc(&h->rec, (size_t)h->n_bulk * BREC * sizeof(double)));
+  if (h->n_bulk) LF_CUDA_H(cudaMalloc(&h->rec, (size_t)h->n_bulk * REC * sizeof(double)));
 
   std::vector<double> S;
   build_S(ad, h->ndp, S);
@@ -480,11 +481,11 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
 
 }  // extern "C"
 
-template <int NDP8, int QC>
+template <int NDP8>
 static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int mask_mass, int te,
                       int eliminate, int rs, cudaStream_t st) {
-  const size_t smem = PmlShape<NDP8, QC>::SMEM;
-  const int threads = PmlShape<NDP8, QC>::THREADS;
+  const size_t smem = PmlShape<NDP8>::SMEM;
+  const int threads = NDP8 * 4;
   auto go = [&](auto kern) -> int {
     LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -497,8 +498,8 @@ static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int ma
     LF_LAUNCHED();
     return LFASM_OK;
   };
-  if (cross) return mode ? go(k_pml_mma<NDP8, QC, true, 1>) : go(k_pml_mma<NDP8, QC, true, 0>);
-  return mode ? go(k_pml_mma<NDP8, QC, false, 1>) : go(k_pml_mma<NDP8, QC, false, 0>);
+  if (cross) return mode ? go(k_pml_mma<NDP8, true, 1>) : go(k_pml_mma<NDP8, true, 0>);
+  return mode ? go(k_pml_mma<NDP8, false, 1>) : go(k_pml_mma<NDP8, false, 0>);
 }
 
 extern "C" {
@@ -529,18 +530,19 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
                                                          h->detJ, h->attr, h->eps_tab,
                                                          h->elem_eps, h->pml, mask, h->rec);
     LF_LAUNCHED();
-    const int ntiles = bulk_tiles(h->ndp);
-    const int ytiles = (ntiles + BULK_WARPS * BULK_T - 1) / (BULK_WARPS * BULK_T);
-    const int nbat = (nb + 7) / 8;
-    // about two waves of resident blocks; each warp keeps its B fragments in
-    // registers across its chunk of element batches
+    const int nthr = bulk_threads(h->ndp);
+    const int ytiles = (nthr + BULK_THREADS - 1) / BULK_THREADS;
+    // about two waves of resident blocks; each block keeps its S-table
+    // values in registers across its chunk of elements
     const long long want = (long long)h->sm_count * 8;
-    const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
-    dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
+    int chunk = (int)std::max<long long>(16, ((long long)nb * ytiles + want - 1) / want);
+    chunk = (chunk + BULK_EB - 1) / BULK_EB * BULK_EB;
+    dim3 grid((nb + chunk - 1) / chunk, ytiles);
 #define LF_BULK(C, M)                                                             \
-  k_bulk<C, M><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                          \
-      nb, h->bulk_list, h->rec, h->S, ntiles, h->nd, h->ndp, h->p, bchunk, te,    \
-      eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
+  k_bulk<C, M><<<grid, BULK_THREADS, 0, h->stream>>>(                             \
+      nb, h->bulk_list, h->rec, h->S, nthr, h->nd, h->ndp, h->p, chunk, te,       \
+      eliminate, rs, (mask & LFASM_CROSS0) ? 1 : 0, (mask & LFASM_CROSS1) ? 1 : 0,  \
+      h->fopack, h->signmask, h->essmask, h->Ae)
     if (cross) { if (mode) LF_BULK(true, 1); else LF_BULK(true, 0); }
     else { if (mode) LF_BULK(false, 1); else LF_BULK(false, 0); }
 #undef LF_BULK
@@ -548,9 +550,9 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[1], h->stream));
   if (h->n_pml) {
-    int rc = h->p == 1 ? launch_pml<8, 4>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
-           : h->p == 2 ? launch_pml<24, 4>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
-                       : launch_pml<48, 8>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst);
+    int rc = h->p == 1 ? launch_pml<8>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
+           : h->p == 2 ? launch_pml<24>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst)
+                       : launch_pml<48>(h, cross, mode, mask_cc, mask_mass, te, eliminate, rs, pst);
     if (rc) return rc;
   }
   if (overlap) {

@@ -37,6 +37,7 @@ struct Rule {
   const double *ip, *w, *v, *c;
 };
 
+constexpr int REC = 28;        // doubles per bulk-element coefficient record
 constexpr int NT_CC = 6;       // symmetric (j <= j') pairs
 constexpr int NT_ALL = 30;     // 6 cc + 6 vv + 9 vc + 9 cv
 constexpr int BULK_THREADS = 128;
@@ -78,26 +79,14 @@ __device__ __forceinline__ int face_of(int k, int p) {
 }
 
 // ---------------------------------------------------------------------------
-// Bulk elements as a tensor-core GEMM.
-//
-// For an element with s == 1 at every quadrature point the element matrix is
-//   A_e = sum_t G_e[t] S_t,   t over 32 terms (30 used):
-//   t  0.. 5  curl-curl, symmetric pairs (00,11,22,01,02,12): G = J^T J / detJ
-//   t  6..11  mass + KLK, same pairs: G = detJ Jinv (-k0^2 eps I - K K) Jinv^T
-//   t 12..20  MixedVectorCurl (j*3+j'):      G = i Jinv K J
-//   t 21..29  MixedVectorWeakCurl (j*3+j'):  G = i J^T K Jinv^T
-// with S_t the element-independent reference quadrature sums.  Written as
-// C (8 elements x 8 entries) = A (8 x 32) B (32 x 8) per m8n8k4 DMMA tile:
-// A = the element coefficient rows (a real row: t 0..11, an imaginary row:
-// t 6..29), B = S in "pair-block-major" entry order n = 4 pb + 2a + b for the
-// 2x2 pair block pb = (I, J) and entry (2I+a, 2J+b).  Each warp keeps the B
-// fragments of its N tiles in registers for the whole kernel.
+// bulk-element coefficient records (REC doubles per element)
+//   [0,6)   gcc: J^T J / detJ at the symmetric pairs (00,11,22,01,02,12)
+//   [6,18)  gvv: detJ Jinv (-k0^2 eps I - K K) Jinv^T, complex, same pairs
+//   [18,27) gx : Jinv K J (the cross coefficients, i factored out), j*3+j'
+// With these, A = Sym + i (c0 X - c1 X^T): Sym = sum gcc Scc + gvv Svv is
+// symmetric and X = sum gx Rvc; the MixedVectorWeakCurl coefficient is
+// J^T K Jinv^T = -(Jinv K J)^T, which turns its term into -X^T.
 // ---------------------------------------------------------------------------
-constexpr int BK = 32;          // coefficient terms (padded)
-constexpr int BREC = 2 * BK;    // doubles per element record: real row, imaginary row
-constexpr int BULK_T = 4;       // N tiles (8 entries) per warp
-constexpr int BULK_WARPS = 4;
-
 __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
                             const double *__restrict__ J9, const double *__restrict__ Ji9,
                             const double *__restrict__ detJ, const int *__restrict__ attr,
@@ -115,9 +104,9 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
   }
   const double det = detJ[e];
   const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
-  double *re = rec + (size_t)i * BREC, *im = re + BK;
+  double *r = rec + (size_t)i * REC;
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-  const bool cc = mask & 1, ms = mask & 2, c0 = mask & 4, c1 = mask & 8, kl = mask & 16;
+  const bool cc = mask & 1, ms = mask & 2, kl = mask & 16;
   const double kx = pml.kx, ky = pml.ky, k2 = pml.k0 * pml.k0;
   // K = [[0,0,ky],[0,0,-kx],[-ky,kx,0]] (fill_K, problem_common.inc:150-158)
   const double K[9] = {0.0, 0.0, ky, 0.0, 0.0, -kx, -ky, kx, 0.0};
@@ -125,10 +114,11 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
   const double mKK[9] = {ky * ky, -kx * ky, 0.0, -kx * ky, kx * kx, 0.0, 0.0, 0.0,
                          kx * kx + ky * ky};
   const double me_re = -k2 * eps.re, me_im = -k2 * eps.im;
-  for (int t = 0; t < BK; ++t) { re[t] = 0.0; im[t] = 0.0; }
   for (int t = 0; t < 6; ++t) {
     const int a = pa[t], b = pb[t];
-    if (cc) re[t] = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
+    double g = 0.0;
+    if (cc) g = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
+    r[t] = g;
     const double jj = Ji[a * 3 + 0] * Ji[b * 3 + 0] + Ji[a * 3 + 1] * Ji[b * 3 + 1] +
                       Ji[a * 3 + 2] * Ji[b * 3 + 2];
     double vr = 0.0, vi = 0.0;
@@ -139,129 +129,161 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
         for (int c2 = 0; c2 < 3; ++c2) s += Ji[a * 3 + rr] * mKK[rr * 3 + c2] * Ji[b * 3 + c2];
       vr += s;
     }
-    re[6 + t] = det * vr;
-    im[6 + t] = det * vi;
+    r[6 + 2 * t] = det * vr;
+    r[7 + 2 * t] = det * vi;
   }
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
-      double gvc = 0.0, gcv = 0.0;
+      double gx = 0.0;
       for (int rr = 0; rr < 3; ++rr)
         for (int c2 = 0; c2 < 3; ++c2) {
           const double k = K[rr * 3 + c2];
-          if (k == 0.0) continue;
-          gvc += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
-          gcv += J[rr * 3 + a] * k * Ji[b * 3 + c2];
+          if (k != 0.0) gx += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
         }
-      if (c0) im[12 + a * 3 + b] = gvc;
-      if (c1) im[21 + a * 3 + b] = gcv;
+      r[18 + a * 3 + b] = gx;
     }
+  r[27] = 0.0;
 }
 
-// ncol_tiles: total N tiles (entries / 8, rounded up); nbatch: element batches
-// of 8.  Block: BULK_WARPS warps, N tiles [blockIdx.y*BULK_WARPS*BULK_T, ...).
+// ---------------------------------------------------------------------------
+// bulk element kernel.  Thread <-> (row pair I, column l >= 2I): it produces
+// A(2I+a, l) and, when l >= 2I+2, the mirrored A(l, 2I+a), a = 0, 1, from NV
+// table values held in registers (symmetric tables at (2I+a, l), cross
+// tables at (2I+a, l) and (l, 2I+a)).  Element records are staged through
+// shared memory in batches of BULK_EB.  Face transforms: the row pair is
+// thread-local, the partner column / row l^1 sits in the neighbouring lane.
+// MODE 0: raw local matrix (ComputeLocal); MODE 1: signs + elimination.
+// ---------------------------------------------------------------------------
+constexpr int BULK_EB = 8;
+
 template <bool CROSS, int MODE>
-__global__ void __launch_bounds__(BULK_WARPS * 32)
+__global__ void __launch_bounds__(BULK_THREADS)
 k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
-       const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
-       int eliminate, int rs, const unsigned *__restrict__ fopack,
+       const double *__restrict__ S, int nthr, int nd, int ndp, int p, int chunk, int te,
+       int eliminate, int rs, int c0, int c1, const unsigned *__restrict__ fopack,
        const unsigned long long *__restrict__ signmask,
        const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
-  __shared__ double sA[8 * BREC];
-  __shared__ int se[8];
-  __shared__ unsigned sfo[8];
-  __shared__ unsigned long long ssm[8], sem[8];
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int g = lane >> 2, t4 = lane & 3;
-  const int H = ndp >> 1, npb = H * H;
-  // B fragments: b[T][k-step] = S[kstep*4 + t4][tile*8 + g]
-  constexpr int KS = BK / 4;
-  double bf[BULK_T][KS];
-  int tile0 = (blockIdx.y * BULK_WARPS + w) * BULK_T;
-#pragma unroll
-  for (int j = 0; j < BULK_T; ++j) {
-    const int tile = tile0 + j;
-#pragma unroll
-    for (int ks = 0; ks < KS; ++ks)
-      bf[j][ks] = tile < ntiles ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
+  constexpr int NV = CROSS ? 60 : 24;
+  __shared__ double sg[BULK_EB * REC];
+  __shared__ int se[BULK_EB];
+  const int tid = threadIdx.x;
+  const int f = blockIdx.y * BULK_THREADS + tid;
+  const bool valid = f < nthr;
+  int I = 0, l = 0;
+  if (valid) {
+    int rem = f;
+    while (rem >= ndp - 2 * I) { rem -= ndp - 2 * I; ++I; }
+    l = 2 * I + rem;
   }
-  // entries owned in the epilogue: n = tile*8 + 2*t4 + {0,1} -> pair block
-  // pb = tile*2 + (t4 >> 1), row half a = t4 & 1, columns 2J, 2J+1
-  const int nbat = (nb + 7) / 8;
-  const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
-  for (int bt = b0; bt < b1; ++bt) {
-    const int ebase = bt * 8;
-    const int nel = min(8, nb - ebase);
+  const bool mirror = valid && l >= 2 * I + 2;
+  const int r0 = 2 * I, r1 = 2 * I + 1;
+  double sv[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) sv[v] = valid ? S[(size_t)v * nthr + f] : 0.0;
+  const int frow = valid ? face_of(r0, p) : -1;
+  const int fcol = valid ? face_of(l & ~1, p) : -1;
+  const int cp = l & 1;
+  const double fc0 = c0 ? 1.0 : 0.0, fc1 = c1 ? 1.0 : 0.0;
+  const int i0 = blockIdx.x * chunk;
+  const int i1 = min(nb, i0 + chunk);
+  for (int ib = i0; ib < i1; ib += BULK_EB) {
+    const int nbat = min(BULK_EB, i1 - ib);
     __syncthreads();
-    for (int j = tid; j < 8 * BREC; j += BULK_WARPS * 32)
-      sA[j] = (j / BREC) < nel ? rec[(size_t)ebase * BREC + j] : 0.0;
-    if (tid < 8) {
-      const int e = tid < nel ? list[ebase + tid] : -1;
-      se[tid] = e;
-      if (e >= 0) {
-        sfo[tid] = fopack[e];
-        if (MODE == 1) {
-          ssm[tid] = signmask[e];
-          sem[tid] = eliminate ? essmask[e] : 0ull;
-        }
+    for (int j = tid; j < nbat * REC; j += BULK_THREADS) sg[j] = rec[(size_t)ib * REC + j];
+    if (tid < nbat) se[tid] = list[ib + tid];
+    __syncthreads();
+    for (int b = 0; b < nbat; ++b) {
+      const double *g = sg + b * REC;
+      double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const double gc = g[t];
+        sr0 = fma(gc, sv[t], sr0);
+        sr1 = fma(gc, sv[12 + t], sr1);
       }
-    }
-    __syncthreads();
-    // A fragments: A[g][kstep*4 + t4] (real row) and imaginary row
-    double ar[3], ai[KS];
 #pragma unroll
-    for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * BREC + ks * 4 + t4];
+      for (int t = 0; t < 6; ++t) {
+        const double gr = g[6 + 2 * t], gi = g[7 + 2 * t];
+        sr0 = fma(gr, sv[6 + t], sr0);
+        si0 = fma(gi, sv[6 + t], si0);
+        sr1 = fma(gr, sv[18 + t], sr1);
+        si1 = fma(gi, sv[18 + t], si1);
+      }
+      // primary A(r0|r1, l) and mirror A(l, r0|r1)
+      double pr0 = sr0, pi0 = si0, pr1 = sr1, pi1 = si1;
+      double mr0 = sr0, mi0 = si0, mr1 = sr1, mi1 = si1;
+      if (CROSS) {
+        double x0 = 0.0, x1 = 0.0, y0 = 0.0, y1 = 0.0;
 #pragma unroll
-    for (int ks = 0; ks < KS; ++ks) ai[ks] = sA[g * BREC + BK + ks * 4 + t4];
-    const int e = se[g];
-#pragma unroll
-    for (int j = 0; j < BULK_T; ++j) {
-      double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
-#pragma unroll
-      for (int ks = 0; ks < 3; ++ks) dmma(cr0, cr1, ar[ks], bf[j][ks]);
-#pragma unroll
-      for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci0, ci1, ai[ks], bf[j][ks]);
-      const int tile = tile0 + j;
-      const int pb = tile * 2 + (t4 >> 1);
-      const int a = t4 & 1;
-      const bool ok = tile < ntiles && pb < npb && e >= 0;
-      const int I = ok ? pb / H : 0, Jp = ok ? pb - I * H : 0;
-      const int row = 2 * I + a, col = 2 * Jp;
-      // dual transform: columns (local pair), rows (partner lane t4^1)
+        for (int t = 0; t < 9; ++t) {
+          const double gx = g[18 + t];
+          x0 = fma(gx, sv[(24 + t) % NV], x0);
+          x1 = fma(gx, sv[(33 + t) % NV], x1);
+          y0 = fma(gx, sv[(42 + t) % NV], y0);
+          y1 = fma(gx, sv[(51 + t) % NV], y1);
+        }
+        pi0 += fc0 * x0 - fc1 * y0;
+        pi1 += fc0 * x1 - fc1 * y1;
+        mi0 += fc0 * y0 - fc1 * x0;
+        mi1 += fc0 * y1 - fc1 * x1;
+      }
+      const int e = se[b];
       if (te && p >= 2) {
-        const unsigned fp = sfo[g];
-        const int fc = face_of(col, p);
-        if (ok && fc >= 0) {
-          const double *T = c_tinv + 4 * ((fp >> (8 * fc)) & 0xffu);
-          const double n0 = T[0] * cr0 + T[1] * cr1, n1 = T[2] * cr0 + T[3] * cr1;
-          const double m0 = T[0] * ci0 + T[1] * ci1, m1 = T[2] * ci0 + T[3] * ci1;
-          cr0 = n0; cr1 = n1; ci0 = m0; ci1 = m1;
+        const unsigned fp = fopack[e];
+        // primary: columns (partner lane holds column l^1), then rows
+        const double qpr0 = __shfl_xor_sync(0xffffffffu, pr0, 1);
+        const double qpi0 = __shfl_xor_sync(0xffffffffu, pi0, 1);
+        const double qpr1 = __shfl_xor_sync(0xffffffffu, pr1, 1);
+        const double qpi1 = __shfl_xor_sync(0xffffffffu, pi1, 1);
+        // mirror: rows l / l^1 across the lane pair, columns local
+        const double qmr0 = __shfl_xor_sync(0xffffffffu, mr0, 1);
+        const double qmi0 = __shfl_xor_sync(0xffffffffu, mi0, 1);
+        const double qmr1 = __shfl_xor_sync(0xffffffffu, mr1, 1);
+        const double qmi1 = __shfl_xor_sync(0xffffffffu, mi1, 1);
+        if (fcol >= 0) {
+          const double *T = c_tinv + 4 * ((fp >> (8 * fcol)) & 0xffu);
+          // M[c'][c] = T[2c + c']: new[cp] = own * T[2cp+cp] + other * T[2cp+1-cp]
+          const double own = T[2 * cp + cp], oth = T[2 * cp + 1 - cp];
+          double n0 = own * pr0 + oth * qpr0, n1 = own * pi0 + oth * qpi0;
+          double n2 = own * pr1 + oth * qpr1, n3 = own * pi1 + oth * qpi1;
+          pr0 = n0; pi0 = n1; pr1 = n2; pi1 = n3;
+          n0 = own * mr0 + oth * qmr0; n1 = own * mi0 + oth * qmi0;
+          n2 = own * mr1 + oth * qmr1; n3 = own * mi1 + oth * qmi1;
+          mr0 = n0; mi0 = n1; mr1 = n2; mi1 = n3;
         }
-        const double qr0 = __shfl_xor_sync(0xffffffffu, cr0, 1);
-        const double qr1 = __shfl_xor_sync(0xffffffffu, cr1, 1);
-        const double qi0 = __shfl_xor_sync(0xffffffffu, ci0, 1);
-        const double qi1 = __shfl_xor_sync(0xffffffffu, ci1, 1);
-        const int fr = face_of(2 * I, p);
-        if (ok && fr >= 0) {
-          const double *T = c_tinv + 4 * ((fp >> (8 * fr)) & 0xffu);
-          const double own = T[2 * a + a], oth = T[2 * a + 1 - a];
-          cr0 = own * cr0 + oth * qr0; cr1 = own * cr1 + oth * qr1;
-          ci0 = own * ci0 + oth * qi0; ci1 = own * ci1 + oth * qi1;
+        if (frow >= 0) {
+          const double *T = c_tinv + 4 * ((fp >> (8 * frow)) & 0xffu);
+          double n0 = T[0] * pr0 + T[1] * pr1, n1 = T[0] * pi0 + T[1] * pi1;
+          double n2 = T[2] * pr0 + T[3] * pr1, n3 = T[2] * pi0 + T[3] * pi1;
+          pr0 = n0; pi0 = n1; pr1 = n2; pi1 = n3;
+          n0 = T[0] * mr0 + T[1] * mr1; n1 = T[0] * mi0 + T[1] * mi1;
+          n2 = T[2] * mr0 + T[3] * mr1; n3 = T[2] * mi0 + T[3] * mi1;
+          mr0 = n0; mi0 = n1; mr1 = n2; mi1 = n3;
         }
       }
-      if (!ok || row >= nd || col >= nd) continue;
-      if (MODE == 1) {
-        const unsigned long long sm = ssm[g], em = sem[g];
-        const double sr = ((sm >> row) & 1ull) ? -1.0 : 1.0;
-        const double s0 = sr * (((sm >> col) & 1ull) ? -1.0 : 1.0);
-        const double s1 = sr * (((sm >> (col + 1)) & 1ull) ? -1.0 : 1.0);
-        cr0 *= s0; ci0 *= s0; cr1 *= s1; ci1 *= s1;
-        const bool er = (em >> row) & 1ull;
-        if (er || ((em >> col) & 1ull)) { cr0 = 0.0; ci0 = 0.0; }
-        if (er || ((em >> (col + 1)) & 1ull)) { cr1 = 0.0; ci1 = 0.0; }
+      if (MODE == 1 && valid) {
+        const unsigned long long sm = signmask[e];
+        const double sl = ((sm >> l) & 1ull) ? -1.0 : 1.0;
+        const double sa = (((sm >> r0) & 1ull) ? -1.0 : 1.0) * sl;
+        const double sb = (((sm >> r1) & 1ull) ? -1.0 : 1.0) * sl;
+        pr0 *= sa; pi0 *= sa; pr1 *= sb; pi1 *= sb;
+        mr0 *= sa; mi0 *= sa; mr1 *= sb; mi1 *= sb;
+        if (eliminate) {
+          const unsigned long long em = essmask[e];
+          const bool el = (em >> l) & 1ull;
+          if (el || ((em >> r0) & 1ull)) { pr0 = pi0 = mr0 = mi0 = 0.0; }
+          if (el || ((em >> r1) & 1ull)) { pr1 = pi1 = mr1 = mi1 = 0.0; }
+        }
       }
-      dcplx *dst = Ae + (size_t)e * nd * rs + (size_t)row * rs + col;
-      dst[0] = mk(cr0, ci0);
-      if (col + 1 < nd) dst[1] = mk(cr1, ci1);
+      if (valid && l < nd) {
+        dcplx *dst = Ae + (size_t)e * nd * rs;
+        dst[(size_t)r0 * rs + l] = mk(pr0, pi0);
+        if (r1 < nd) dst[(size_t)r1 * rs + l] = mk(pr1, pi1);
+        if (mirror) {
+          dst[(size_t)l * rs + r0] = mk(mr0, mi0);
+          if (r1 < nd) dst[(size_t)l * rs + r1] = mk(mr1, mi1);
+        }
+      }
     }
   }
 }
@@ -278,7 +300,7 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 // M tiles, so the epilogue holds both parts of each entry.  Rows are staged
 // in chunks of PML_QC points; blocks are persistent over the PML elements.
 // ---------------------------------------------------------------------------
-constexpr int PML_QMAX = 8;  // max quadrature points per staged chunk (blockDim = QC * NDP8)
+constexpr int PML_QC = 8;  // quadrature points staged per round
 
 struct QCoef {  // per quadrature point, already multiplied by w_q detJ
   dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries (cc rule: Lambda^-1 diagonal)
@@ -286,64 +308,17 @@ struct QCoef {  // per quadrature point, already multiplied by w_q detJ
   dcplx c02, c12, c20, c21;           // M1 = i Lambda^-1 K
 };
 
-template <int NDP8, int QC>
+template <int NDP8>
 struct PmlShape {
-  static constexpr int NW = NDP8 / 8;                    // column tiles
+  static constexpr int NW = NDP8 / 8;                    // warps = column tiles
   static constexpr int MT = NDP8 / 8;                    // row tiles
-  static constexpr int WPC = QC / 4;                     // warps per column tile
-  static constexpr int MTW = MT / WPC;                   // row tiles per warp
-  static_assert(MT % WPC == 0, "row tiles must split evenly");
-  static constexpr int THREADS = QC * NDP8;
   static constexpr int LD = (NDP8 % 16 == 0) ? NDP8 + 8 : NDP8;  // row stride = 8 mod 16
-  static constexpr int RMAX = QC * 6;                    // rows per chunk (multiple of 4)
-  static constexpr int BUF = 3 * RMAX * LD;              // X, Yre, Yim of one chunk
-  static constexpr size_t SMEM = (size_t)2 * BUF * sizeof(double) + 2 * QC * sizeof(QCoef);
+  static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
+  static constexpr size_t SMEM = (size_t)3 * RMAX * LD * sizeof(double) + PML_QC * sizeof(QCoef);
 };
 
-__device__ __forceinline__ void pml_coef(QCoef &c, int rule, int mask, const Rule &R, int q,
-                                         const double *sJ, double sv0z, double sdet,
-                                         dcplx seps, const PmlParams &pml) {
-  const double k2 = pml.k0 * pml.k0;
-  const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
-  const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
-                   sJ[8] * R.ip[q * 3 + 2];
-  const dcplx s = pml_s(pml, z);
-  const dcplx si = cinv(s);
-  const double wq = R.w[q] * sdet;
-  if (rule == 0) {
-    c.a00 = cscale(wq, si); c.a11 = cscale(wq, si); c.a22 = cscale(wq, s);
-    c.a01 = mk(0, 0); c.a10 = mk(0, 0);
-    c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
-    return;
-  }
-  const dcplx li0 = si, li1 = si, li2 = s;
-  dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
-  if (mask & 2) {
-    const dcplx me = cscale(-k2, seps);
-    a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
-  }
-  if (mask & 16) {
-    a00 = cadd(a00, cscale(-K02 * K20, li2));
-    a01 = cadd(a01, cscale(-K02 * K21, li2));
-    a10 = cadd(a10, cscale(-K12 * K20, li2));
-    a11 = cadd(a11, cscale(-K12 * K21, li2));
-    a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
-  }
-  c.a00 = cscale(wq, a00); c.a01 = cscale(wq, a01); c.a10 = cscale(wq, a10);
-  c.a11 = cscale(wq, a11); c.a22 = cscale(wq, a22);
-  const dcplx iu = mk(0.0, 1.0);
-  if (mask & 4) {
-    c.b02 = cscale(wq * K02, cmul(iu, li2)); c.b12 = cscale(wq * K12, cmul(iu, li2));
-    c.b20 = cscale(wq * K20, cmul(iu, li0)); c.b21 = cscale(wq * K21, cmul(iu, li1));
-  } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
-  if (mask & 8) {
-    c.c02 = cscale(wq * K02, cmul(iu, li0)); c.c12 = cscale(wq * K12, cmul(iu, li1));
-    c.c20 = cscale(wq * K20, cmul(iu, li2)); c.c21 = cscale(wq * K21, cmul(iu, li2));
-  } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
-}
-
-template <int NDP8, int QC, bool CROSS, int MODE>
-__global__ void __launch_bounds__(NDP8 * QC)
+template <int NDP8, bool CROSS, int MODE>
+__global__ void __launch_bounds__(NDP8 * 4)
 k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
           const double *__restrict__ J9, const double *__restrict__ Ji9,
           const double *__restrict__ detJ, const double *__restrict__ v0,
@@ -352,122 +327,26 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
           int te, int eliminate, const unsigned *__restrict__ fopack,
           const unsigned long long *__restrict__ signmask,
           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
-  using Sh = PmlShape<NDP8, QC>;
-  constexpr int LD = Sh::LD, RMAX = Sh::RMAX, BUF = Sh::BUF, NW = Sh::NW, MTW = Sh::MTW;
-  constexpr int PML_QC = QC;
+  using Sh = PmlShape<NDP8>;
+  constexpr int LD = Sh::LD, MT = Sh::MT, RMAX = Sh::RMAX;
   extern __shared__ double smem[];
-  QCoef *qcb = reinterpret_cast<QCoef *>(smem + 2 * BUF);  // [2][PML_QC]
+  double *Xs = smem;
+  double *Yr = Xs + RMAX * LD;
+  double *Yi = Yr + RMAX * LD;
+  QCoef *qc = reinterpret_cast<QCoef *>(Yi + RMAX * LD);
   __shared__ double sJ[9], sJi[9], sdet, sv0z;
   __shared__ dcplx seps;
   __shared__ unsigned sfo;
 
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
-  const int w = wid % NW;               // column tile of this warp
-  const int mbase = (wid / NW) * MTW;   // first row tile of this warp
-  // staging item of this thread: quadrature point qi of the chunk, column k
-  const int qi = tid / NDP8, k = tid - qi * NDP8;
-  const bool cross_on = CROSS && (mask_mass & (4 | 8));
-  const int ncc = mask_cc ? (rcc.nq + PML_QC - 1) / PML_QC : 0;
-  const int nms = mask_mass ? (rm.nq + PML_QC - 1) / PML_QC : 0;
-  const int nch = ncc + nms;
-
-  auto chunk_info = [&](int c, int &rule, int &q0, int &nqc, int &rq) {
-    rule = c < ncc ? 0 : 1;
-    q0 = (rule == 0 ? c : c - ncc) * PML_QC;
-    const int nq = rule == 0 ? rcc.nq : rm.nq;
-    nqc = min(PML_QC, nq - q0);
-    rq = rule == 0 ? 3 : (cross_on ? 6 : 3);
-  };
-  auto coefs = [&](int c) {
-    if (c >= nch) return;
-    int rule, q0, nqc, rq;
-    chunk_info(c, rule, q0, nqc, rq);
-    if (tid < nqc)
-      pml_coef(qcb[(c & 1) * PML_QC + tid], rule, rule == 0 ? mask_cc : mask_mass,
-               rule == 0 ? rcc : rm, q0 + tid, sJ, sv0z, sdet, seps, pml);
-  };
-  auto stage = [&](int c) {
-    if (c >= nch) return;
-    int rule, q0, nqc, rq;
-    chunk_info(c, rule, q0, nqc, rq);
-    double *Xs = smem + (c & 1) * BUF, *Yr = Xs + RMAX * LD, *Yi = Yr + RMAX * LD;
-    const Rule &R = rule == 0 ? rcc : rm;
-    const bool need_c = rule == 0 || cross_on;
-    const bool need_v = rule == 1;
-    const bool live = qi < nqc;
-    double v[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
-    if (live && k < nd) {
-      const int q = q0 + qi;
-      const double *rv = R.v + ((size_t)q * nd + k) * 3;
-      const double *rc = R.c + ((size_t)q * nd + k) * 3;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (need_v) v[d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
-        if (need_c) cv[d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
-      }
-    }
-    if (te && p >= 2) {  // face pair (k, k^1) lives in the neighbouring lane
-      double pv[3], pc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        pv[d] = __shfl_xor_sync(0xffffffffu, v[d], 1);
-        pc[d] = __shfl_xor_sync(0xffffffffu, cv[d], 1);
-      }
-      const int f = face_of(k & ~1, p);
-      if (f >= 0) {
-        const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
-        const int h = k & 1;
-        const double own = T[2 * h + h], oth = T[2 * h + 1 - h];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          v[d] = own * v[d] + oth * pv[d];
-          cv[d] = own * cv[d] + oth * pc[d];
-        }
-      }
-    }
-    const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
-    // zero the padding rows up to a multiple of 4
-    for (int i = tid; i < (nrows4 - nrows) * NDP8; i += blockDim.x) {
-      const int r = nrows + i / NDP8, kk = i % NDP8;
-      Xs[r * LD + kk] = 0.0; Yr[r * LD + kk] = 0.0; Yi[r * LD + kk] = 0.0;
-    }
-    if (!live) return;
-    const QCoef &C = qcb[(c & 1) * PML_QC + qi];
-    const int rb = qi * rq;
-    if (rule == 0) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = cv[d];
-      Yr[(rb + 0) * LD + k] = cv[0] * C.a00.re; Yi[(rb + 0) * LD + k] = cv[0] * C.a00.im;
-      Yr[(rb + 1) * LD + k] = cv[1] * C.a11.re; Yi[(rb + 1) * LD + k] = cv[1] * C.a11.im;
-      Yr[(rb + 2) * LD + k] = cv[2] * C.a22.re; Yi[(rb + 2) * LD + k] = cv[2] * C.a22.im;
-      return;
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = v[d];
-    dcplx y0 = cadd(cscale(v[0], C.a00), cscale(v[1], C.a01));
-    dcplx y1 = cadd(cscale(v[0], C.a10), cscale(v[1], C.a11));
-    dcplx y2 = cscale(v[2], C.a22);
-    if (cross_on) {
-      y0 = cadd(y0, cscale(cv[2], C.b02));
-      y1 = cadd(y1, cscale(cv[2], C.b12));
-      y2 = cadd(y2, cadd(cscale(cv[0], C.b20), cscale(cv[1], C.b21)));
-#pragma unroll
-      for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cv[d];
-      const dcplx z0 = cscale(v[2], C.c02), z1 = cscale(v[2], C.c12),
-                  z2 = cadd(cscale(v[0], C.c20), cscale(v[1], C.c21));
-      Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
-      Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
-      Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
-    }
-    Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-    Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-    Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
-  };
+  const double k2 = pml.k0 * pml.k0;
+  const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
+  constexpr int npair = NDP8 / 2;
 
   for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
     const int e = list[ie];
-    __syncthreads();  // previous element done with shared state
+    __syncthreads();  // previous element done with the shared scalars
     if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
     if (tid == 0) {
       sdet = detJ[e];
@@ -475,33 +354,154 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
       seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
       sfo = fopack[e];
     }
-    double cr[MTW][2], ci[MTW][2];
+    double cr[MT][2], ci[MT][2];
 #pragma unroll
-    for (int m = 0; m < MTW; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
+    for (int m = 0; m < MT; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
     __syncthreads();
-    coefs(0);
-    __syncthreads();
-    stage(0);
-    coefs(1);
-    __syncthreads();
-    for (int c = 0; c < nch; ++c) {
-      stage(c + 1);
-      coefs(c + 2);
-      int rule, q0, nqc, rq;
-      chunk_info(c, rule, q0, nqc, rq);
-      const int nrows4 = (nqc * rq + 3) & ~3;
-      const double *Xs = smem + (c & 1) * BUF, *Yr = Xs + RMAX * LD, *Yi = Yr + RMAX * LD;
-      for (int r0 = 0; r0 < nrows4; r0 += 4) {
-        const double br = Yr[(r0 + t4) * LD + w * 8 + g];
-        const double bi = Yi[(r0 + t4) * LD + w * 8 + g];
-#pragma unroll
-        for (int m = 0; m < MTW; ++m) {
-          const double a = Xs[(r0 + t4) * LD + (mbase + m) * 8 + g];
-          dmma(cr[m][0], cr[m][1], a, br);
-          dmma(ci[m][0], ci[m][1], a, bi);
+
+    for (int rule = 0; rule < 2; ++rule) {
+      const int mask = rule == 0 ? mask_cc : mask_mass;
+      if (!mask) continue;
+      const Rule R = rule == 0 ? rcc : rm;
+      const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+      const bool need_v = rule == 1;
+      const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+      for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
+        const int nqc = min(PML_QC, R.nq - q0);
+        const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
+        if (tid < nqc) {
+          const int q = q0 + tid;
+          const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
+                           sJ[8] * R.ip[q * 3 + 2];
+          const dcplx s = pml_s(pml, z);
+          const dcplx si = cinv(s);
+          const double wq = R.w[q] * sdet;
+          QCoef c;
+          if (rule == 0) {
+            c.a00 = cscale(wq, si); c.a11 = cscale(wq, si); c.a22 = cscale(wq, s);
+            c.a01 = mk(0, 0); c.a10 = mk(0, 0);
+            c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
+          } else {
+            const dcplx li0 = si, li1 = si, li2 = s;
+            dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
+            if (mask & 2) {
+              const dcplx me = cscale(-k2, seps);
+              a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
+            }
+            if (mask & 16) {
+              a00 = cadd(a00, cscale(-K02 * K20, li2));
+              a01 = cadd(a01, cscale(-K02 * K21, li2));
+              a10 = cadd(a10, cscale(-K12 * K20, li2));
+              a11 = cadd(a11, cscale(-K12 * K21, li2));
+              a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
+            }
+            c.a00 = cscale(wq, a00); c.a01 = cscale(wq, a01); c.a10 = cscale(wq, a10);
+            c.a11 = cscale(wq, a11); c.a22 = cscale(wq, a22);
+            const dcplx iu = mk(0.0, 1.0);
+            if (mask & 4) {
+              c.b02 = cscale(wq * K02, cmul(iu, li2)); c.b12 = cscale(wq * K12, cmul(iu, li2));
+              c.b20 = cscale(wq * K20, cmul(iu, li0)); c.b21 = cscale(wq * K21, cmul(iu, li1));
+            } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
+            if (mask & 8) {
+              c.c02 = cscale(wq * K02, cmul(iu, li0)); c.c12 = cscale(wq * K12, cmul(iu, li1));
+              c.c20 = cscale(wq * K20, cmul(iu, li2)); c.c21 = cscale(wq * K21, cmul(iu, li2));
+            } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
+          }
+          qc[tid] = c;
         }
+        // zero the padding rows up to a multiple of 4
+        for (int i = tid; i < (nrows4 - nrows) * LD; i += blockDim.x) {
+          const int r = nrows + i / LD, k = i % LD;
+          Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+        }
+        __syncthreads();
+        for (int it = tid; it < nqc * npair; it += blockDim.x) {
+          const int qi = it / npair, pr = it - qi * npair;
+          const int q = q0 + qi;
+          double v[2][3], c[2][3];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * pr + h;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
+            if (k < nd) {
+              const double *rv = R.v + ((size_t)q * nd + k) * 3;
+              const double *rc = R.c + ((size_t)q * nd + k) * 3;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                if (need_v)
+                  v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
+                if (need_c)
+                  c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
+              }
+            }
+          }
+          if (te && p >= 2) {
+            const int f = face_of(2 * pr, p);
+            if (f >= 0) {
+              const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
+                v[0][d] = v0_ * T[0] + v1_ * T[1];
+                v[1][d] = v0_ * T[2] + v1_ * T[3];
+                c[0][d] = c0_ * T[0] + c1_ * T[1];
+                c[1][d] = c0_ * T[2] + c1_ * T[3];
+              }
+            }
+          }
+          const QCoef &C = qc[qi];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * pr + h;
+            const int rb = qi * rq;
+            if (rule == 0) {
+#pragma unroll
+              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
+              const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
+                          y2 = cscale(c[h][2], C.a22);
+              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+            } else {
+              const double *vv = v[h], *cc = c[h];
+#pragma unroll
+              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
+              dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+              dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+              dcplx y2 = cscale(vv[2], C.a22);
+              if (need_c) {
+                y0 = cadd(y0, cscale(cc[2], C.b02));
+                y1 = cadd(y1, cscale(cc[2], C.b12));
+                y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
+                const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
+                            z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+                Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
+                Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
+                Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
+              }
+              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+            }
+          }
+        }
+        __syncthreads();
+        // tensor-core contraction of the staged rows
+        for (int r0 = 0; r0 < nrows4; r0 += 4) {
+          const double br = Yr[(r0 + t4) * LD + w * 8 + g];
+          const double bi = Yi[(r0 + t4) * LD + w * 8 + g];
+#pragma unroll
+          for (int m = 0; m < MT; ++m) {
+            const double a = Xs[(r0 + t4) * LD + m * 8 + g];
+            dmma(cr[m][0], cr[m][1], a, br);
+            dmma(ci[m][0], ci[m][1], a, bi);
+          }
+        }
+        __syncthreads();
       }
-      __syncthreads();
     }
     // epilogue: C[row = m*8 + g][col = w*8 + 2*t4 + i]
     const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
@@ -509,8 +509,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
     dcplx *dst = Ae + (size_t)e * nd * rs;
     const int col = w * 8 + 2 * t4;
 #pragma unroll
-    for (int m = 0; m < MTW; ++m) {
-      const int row = (mbase + m) * 8 + g;
+    for (int m = 0; m < MT; ++m) {
+      const int row = m * 8 + g;
       if (row >= nd) continue;
       dcplx v2[2];
 #pragma unroll
