@@ -182,6 +182,22 @@ int lfasm_residual(lfasm_handle *h, const double *X, const double *B, double *re
 int lfasm_residual_device(lfasm_handle *h, const void *d_x, const void *d_b,
                           double *rel);
 
+/* Allocation-free residual (no counterpart in the reference): ||A x - b|| /
+ * ||b|| for a device CSR given by plain pointers (int32 row pointer and
+ * columns, interleaved complex128 values, x and b of length n), computed on
+ * `stream` (a cudaStream_t; NULL = default) of the current device and
+ * returned in *rel.  For callers that cannot call cudaMalloc while they run
+ * (a solver loop whose memory is all held by its factorization, or a host
+ * framework that owns every device allocation): it allocates nothing.  Its
+ * partial sums use a fixed 4 MiB device array inside the library, which
+ * bounds n to 2,097,152 rows (larger n fails with LFASM_ERR_UNSUPPORTED).
+ * The first call on a device looks up that array's address, so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be
+ * serialized by the caller. */
+int lfasm_csr_residual_noalloc(int n, const int *d_rowptr, const int *d_cols, const void *d_vals,
+                               const void *d_x, const void *d_b, double *rel, void *stream);
+
 /* y = A x on device vectors (interleaved complex128, length n). */
 int lfasm_spmv(lfasm_handle *h, const void *d_x, void *d_y);
 

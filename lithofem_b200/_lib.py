@@ -59,6 +59,9 @@ def lib() -> ct.CDLL:
         "lfasm_path_counts": (ct.c_int, [H, c_int_p, c_int_p]),
         "lfasm_set_profile": (ct.c_int, [H, ct.c_int]),
         "lfasm_stage_times": (ct.c_int, [H, ct.POINTER(ct.c_float)]),
+        "lfasm_csr_residual_noalloc": (ct.c_int, [ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                                  ct.c_void_p, ct.c_void_p, c_double_p,
+                                                  ct.c_void_p]),
         "lfasm_destroy": (None, [H]),
     }
     for name, (res, args) in sig.items():

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -856,6 +857,79 @@ int lfasm_residual_device(lfasm_handle *h, const void *d_x, const void *d_b, dou
   if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
   LF_CUDA(cudaSetDevice(h->dev));
   return residual_core(h, (const dcplx *)d_x, (const dcplx *)d_b, rel);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual.
+//
+// For callers that must not allocate device memory once they are running:
+// a solver loop that has handed all remaining memory to its factorization,
+// or a host framework whose own pool owns every device allocation and
+// forbids side allocations.  The partial sums of the residual live in this
+// file-scope device array instead of memory from cudaMalloc; every GPU that
+// loads the library keeps it (64 KiB per 4096 blocks, 4 MiB in total) until
+// the process exits.  Host code must not pass the symbol itself to a kernel
+// (on the host it only names a stand-in object): its device address is
+// looked up once per device with cudaGetSymbolAddress, on the first call
+// made on that device.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int NOALLOC_WPB = 8;                    // rows (warps) per block
+constexpr int NOALLOC_MAX_BLOCKS = 1 << 18;       // 262144 blocks
+static __device__ __align__(256) double g_noalloc_scratch[2 * NOALLOC_MAX_BLOCKS + 2];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(int dev, double **out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (dev < 0 || dev >= 64) return fail(LFASM_ERR_UNSUPPORTED, "device ordinal %d >= 64", dev);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    LF_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return LFASM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lfasm_csr_residual_noalloc(int n, const int *d_rowptr, const int *d_cols, const void *d_vals,
+                               const void *d_x, const void *d_b, double *rel, void *stream) {
+  g_err.clear();
+  if (!rel) return fail(LFASM_ERR_ARG, "NULL result pointer");
+  if (n < 0) return fail(LFASM_ERR_ARG, "negative row count %d", n);
+  const long long max_rows = (long long)NOALLOC_WPB * NOALLOC_MAX_BLOCKS;
+  if (n > max_rows)
+    return fail(LFASM_ERR_UNSUPPORTED,
+                "n = %d rows exceeds the allocation-free residual limit of %lld rows", n, max_rows);
+  if (n == 0) { *rel = 0.0; return LFASM_OK; }
+  if (!d_rowptr || !d_cols || !d_vals || !d_x || !d_b) return fail(LFASM_ERR_ARG, "NULL argument");
+  int dev = 0;
+  LF_CUDA(cudaGetDevice(&dev));
+  double *scratch = nullptr;
+  int rc = noalloc_scratch(dev, &scratch);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (n + NOALLOC_WPB - 1) / NOALLOC_WPB;
+  // every block writes its own partial pair and k_sum_partials overwrites
+  // the two result slots: nothing carries over from an earlier call
+  k_spmv_resid<<<nb, NOALLOC_WPB * 32, 0, st>>>(n, d_rowptr, d_cols, (const dcplx *)d_vals,
+                                                 (const dcplx *)d_x, (const dcplx *)d_b, nullptr,
+                                                 scratch);
+  LF_LAUNCHED();
+  k_sum_partials<<<1, 1024, 0, st>>>(nb, scratch, scratch + 2 * NOALLOC_MAX_BLOCKS);
+  LF_LAUNCHED();
+  double hr[2];
+  LF_CUDA(cudaMemcpyAsync(hr, scratch + 2 * NOALLOC_MAX_BLOCKS, sizeof(hr),
+                          cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaStreamSynchronize(st));
+  *rel = hr[1] > 0.0 ? std::sqrt(hr[0] / hr[1]) : 0.0;
+  return LFASM_OK;
 }
 
 int lfasm_spmv(lfasm_handle *h, const void *d_x, void *d_y) {
