@@ -373,7 +373,8 @@ def run_ours(a, rank, world, local, dist, torch):
     top = int(np.argmax(stages))
     if top == 1:
         ach = kern["pml"]["TFLOP/s"]
-        roof = {"kernel": "k_pml (PML elements, FP64 quadrature contraction)", "bound": "fp64",
+        roof = {"kernel": "k_pml_mma", "what": "PML elements, FP64 quadrature contraction on DMMA",
+                "bound": "tensor",
                 "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
                 "peak_source": "measured in-run: cuBLAS DGEMM 8192^3", "traffic": None}
     else:
@@ -382,11 +383,12 @@ def run_ours(a, rank, world, local, dist, torch):
         roof = {"kernel": {"prep+bulk": "k_bulk", "gather": "k_gather"}[nm], "bound": "hbm",
                 "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
-    prof_path = ROOT / "profiles" / "traffic.json"
-    if prof_path.exists():
+    prof_path = ROOT / "profiles" / "traffic_c3_line_grating_p3.json"
+    if prof_path.exists() and a.config == 3 and a.scale == 1.0:
         try:
             tr = json.loads(prof_path.read_text())
-            roof["traffic"] = tr.get(roof["kernel"].split()[0])
+            roof["traffic"] = tr.get(roof["kernel"])
+            roof["traffic_source"] = "profiles/traffic_c3_line_grating_p3.json (ncu, scaled)"
         except Exception:
             pass
 
