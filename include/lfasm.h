@@ -213,6 +213,18 @@ int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts,
                        int n_parts, const int *col_of_part, int ncol,
                        int eliminate, void *d_b);
 
+/* Adjoint contraction for per-element permittivity.  For a linear
+ * functional l(u) = c^T u of the solution of A(eps) u = b(eps) and the
+ * adjoint solution A^T lambda = c (device vectors, interleaved complex128),
+ * writes d_grad[e] = dl/deps_e = lambda^T (db/deps_e - dA/deps_e u) for
+ * every non-PML element (0 for PML elements; ne complex128 entries):
+ * dA_e/deps_e = -k0^2 M_e (the Lambda-weighted mass matrix of the mass
+ * integrator, problem_common.inc:123-148) and db_e/deps_e = k0^2 int v.Ehat
+ * (ScatterSource, problem_common.inc:238-266) with the incident parts of the
+ * source (summed).  No counterpart in the reference (it has no adjoint). */
+int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_parts,
+                       const void *d_u, const void *d_lambda, void *d_grad);
+
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
  * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the

@@ -62,6 +62,8 @@ def lib() -> ct.CDLL:
         "lfasm_csr_residual_noalloc": (ct.c_int, [ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                                   ct.c_void_p, ct.c_void_p, c_double_p,
                                                   ct.c_void_p]),
+        "lfasm_eps_gradient": (ct.c_int, [H, ct.POINTER(IncidentPartC), ct.c_int, ct.c_void_p,
+                                          ct.c_void_p, ct.c_void_p]),
         "lfasm_destroy": (None, [H]),
     }
     for name, (res, args) in sig.items():

@@ -1,0 +1,139 @@
+"""Adjoint gradient of a far-field objective with respect to per-element eps.
+
+Objective: J = |l(u)|^2 with l(u) = c^T u the plane mean of one component of
+the scattered envelope on a sampling plane, i.e. the (0,0) Rayleigh
+coefficient of that component (the reference takes orders as plane FFTs,
+src/lithofem/orders.py:36-67; the (0,0) term is the mean), and u the
+solution of A(eps) u = b(eps) assembled by liblfasm.
+
+Gradient (A, b holomorphic in eps_e):  with A^T lambda = c,
+    dl/deps_e = lambda^T (db/deps_e - dA/deps_e u)      (lfasm_eps_gradient)
+    dJ/dRe eps_e = 2 Re(conj(l) dl/deps_e),  dJ/dIm eps_e = -2 Im(conj(l) dl/deps_e).
+
+The sparse solves are delegated to a solver object with ``solve(b)`` and
+``solve_transposed(c)``; ``HostLU`` is a stand-in for the cuDSS factorisation
+the reference uses (not present in this image): it factors the device CSR
+once on the host with SuperLU and reuses the factors for the transposed
+solve.  The assembly, right-hand side and gradient contraction run on the
+GPU (liblfasm).
+"""
+
+from __future__ import annotations
+
+import copy
+
+import numpy as np
+
+from . import ndbasis, space
+from .asm import AsmGpuGlobal
+
+
+class HostLU:
+    """SuperLU factorisation of the device CSR (stand-in for cuDSS)."""
+
+    def __init__(self, g: AsmGpuGlobal):
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+        I, J = g.DownloadCsr()
+        n = len(I) - 1
+        A = sp.csr_matrix((g.DownloadValues(), J, I), shape=(n, n))
+        self.lu = spl.splu(A.tocsc())
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        return self.lu.solve(b)
+
+    def solve_transposed(self, c: np.ndarray) -> np.ndarray:
+        return self.lu.solve(c, trans="T")
+
+
+def plane_functional(ad: space.AsmData, z: float, lx: float, ly: float, comp: int,
+                     nx: int = 8, ny: int = 8) -> np.ndarray:
+    """c with c^T u = mean over an nx x ny plane grid of u_comp(x, y, z)."""
+    xs = (np.arange(nx) + 0.5) * lx / nx
+    ys = (np.arange(ny) + 0.5) * ly / ny
+    X = np.array([[x, y, z] for y in ys for x in xs])
+    ne, nd, p = ad.ne, ad.nd, ad.p
+    Ji = ad.Jinv.reshape(ne, 3, 3)
+    v0 = ad.v0.reshape(ne, 3)
+    dof = ad.dof.reshape(ne, nd)
+    sg = ad.sign.reshape(ne, nd)
+    fo = ad.fo.reshape(ne, 4) if p > 1 else None
+    el = ndbasis.nd_element(p)
+    c = np.zeros(ad.height, dtype=complex)
+    for x in X:
+        xi = np.einsum("eij,ej->ei", Ji, x[None, :] - v0)
+        lam = np.column_stack([1 - xi.sum(1), xi])
+        e = int(np.argmax((lam >= -1e-12).all(1)))
+        phys = el.vshape(xi[e][None])[0] @ Ji[e]          # (nd, 3) local basis values
+        w = phys[:, comp] / len(X)                        # weight of local coefficient k
+        # local coefficient = M (sign * global): fold M^T and the sign
+        wg = w.copy()
+        if p > 1:
+            for f in range(4):
+                M = space.face_tinv(fo[e, f])
+                for i in range(p * (p - 1) // 2):
+                    d0 = 6 * p + f * p * (p - 1) + 2 * i
+                    wg[d0:d0 + 2] = M.T @ w[d0:d0 + 2]
+        np.add.at(c, dof[e], sg[e] * wg)
+    return c
+
+
+class EpsAdjoint:
+    """Assemble, solve and differentiate J = |c^T u|^2 w.r.t. per-element eps."""
+
+    def __init__(self, ad, prob, parts, c: np.ndarray, gpu_id: int = 0, solver=HostLU):
+        self.ad, self.prob0, self.parts, self.c = ad, prob, parts, c
+        self.gpu_id, self.solver_cls = gpu_id, solver
+
+    def _assemble(self, eps: np.ndarray):
+        import torch
+        prob = copy.copy(self.prob0)
+        prob.elem_eps = np.asarray(eps, dtype=complex)
+        g = AsmGpuGlobal(prob)
+        assert g.Init(self.ad, self.gpu_id) and g.BuildGlobal(self.ad.ess) and g.Assemble(True)
+        b = torch.zeros(self.ad.height, dtype=torch.complex128, device=f"cuda:{self.gpu_id}")
+        assert g.AssembleRHS(self.parts, [0] * len(self.parts), 1, True, b.data_ptr())
+        return g, b
+
+    def value(self, eps: np.ndarray) -> complex:
+        g, b = self._assemble(eps)
+        u = self.solver_cls(g).solve(b.cpu().numpy())
+        return complex(self.c @ u)
+
+    def value_and_grad(self, eps: np.ndarray):
+        """(l, J, dJ/dRe eps, dJ/dIm eps, dl/deps) for eps (ne complex)."""
+        import torch
+        g, b = self._assemble(eps)
+        lu = self.solver_cls(g)
+        u = lu.solve(b.cpu().numpy())
+        lam = lu.solve_transposed(self.c)
+        ell = complex(self.c @ u)
+        dev = b.device
+        ud = torch.from_numpy(u).to(dev)
+        ld = torch.from_numpy(lam).to(dev)
+        gd = torch.zeros(self.ad.ne, dtype=torch.complex128, device=dev)
+        assert g.EpsGradient(self.parts, ud.data_ptr(), ld.data_ptr(), gd.data_ptr())
+        dl = gd.cpu().numpy()
+        dJ_re = 2.0 * np.real(np.conj(ell) * dl)
+        dJ_im = -2.0 * np.imag(np.conj(ell) * dl)
+        return ell, abs(ell) ** 2, dJ_re, dJ_im, dl
+
+
+def autograd_function(adj: EpsAdjoint):
+    """torch.autograd.Function mapping (Re eps, Im eps) -> J = |l|^2."""
+    import torch
+
+    class _EpsObjective(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, eps_re, eps_im):
+            eps = eps_re.detach().cpu().numpy() + 1j * eps_im.detach().cpu().numpy()
+            _, J, gre, gim, _ = adj.value_and_grad(eps)
+            ctx.save_for_backward(torch.from_numpy(gre).to(eps_re), torch.from_numpy(gim).to(eps_im))
+            return eps_re.new_tensor(J)
+
+        @staticmethod
+        def backward(ctx, gout):
+            gre, gim = ctx.saved_tensors
+            return gout * gre, gout * gim
+
+    return _EpsObjective

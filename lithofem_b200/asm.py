@@ -194,6 +194,14 @@ class AsmGpuGlobal(AsmGpu):
     def SpMV(self, x_ptr: int, y_ptr: int) -> bool:
         return self._ok(_lib.lib().lfasm_spmv(self._h, ct.c_void_p(x_ptr), ct.c_void_p(y_ptr)))
 
+    def EpsGradient(self, parts, u_ptr: int, lam_ptr: int, grad_ptr: int) -> bool:
+        """grad[e] = lambda^T (db/deps_e - dA/deps_e u) for the non-PML elements."""
+        arr, keep = marshal_parts(parts)
+        ok = self._ok(_lib.lib().lfasm_eps_gradient(self._h, arr, len(parts), ct.c_void_p(u_ptr),
+                                                    ct.c_void_p(lam_ptr), ct.c_void_p(grad_ptr)))
+        del keep
+        return ok
+
     def AssembleRHS(self, parts, col_of_part, ncol: int, eliminate: bool, b_ptr: int) -> bool:
         arr, keep = marshal_parts(parts)
         cols = np.ascontiguousarray(np.asarray(col_of_part, dtype=np.int32))

@@ -108,6 +108,7 @@ struct lfasm_handle {
   int *src_list = nullptr, *src_slot = nullptr;
   int n_src = 0;
   int max_src_slab = -1;  // largest slab index among RHS source elements
+  int max_bulk_slab = -1; // largest slab index among the non-PML (design) elements
   // global
   int built = 0, locals_valid = 0;
   int *I = nullptr, *Jc = nullptr;
@@ -441,6 +442,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
       }
     }
     h->n_src = (int)src.size();
+    for (int e : bl) h->max_bulk_slab = std::max(h->max_bulk_slab, slab[e]);
     LF_CUDA_H(upload(h->slab_of, slab.data(), ne));
     LF_CUDA_H(upload(h->delta, del.data(), ne));
     LF_CUDA_H(upload(h->src_list, src.data(), src.size()));
@@ -996,6 +998,59 @@ int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts, int n_
   cudaFree(dw);
   if (dcol) cudaFree(dcol);
   if (be) cudaFree(be);
+  return sync_if(h);
+}
+
+static int upload_waves(const lfasm_incident_part *parts, int n_parts, int n_slab_min,
+                        std::vector<SlabWaveD> &waves, int &n_slab) {
+  n_slab = n_parts > 0 ? parts[0].n_slab : 1;
+  if (n_parts > 0 && n_slab_min >= n_slab)
+    return fail(LFASM_ERR_ARG, "incident tables have %d slabs; elements reach slab %d", n_slab,
+                n_slab_min);
+  waves.assign((size_t)std::max(n_parts, 1) * n_slab, SlabWaveD{});
+  for (int pi = 0; pi < n_parts; ++pi) {
+    const lfasm_incident_part &P = parts[pi];
+    if (P.n_slab != n_slab) return fail(LFASM_ERR_ARG, "parts disagree on the slab count");
+    for (int s = 0; s < n_slab; ++s) {
+      SlabWaveD &w = waves[(size_t)pi * n_slab + s];
+      w.qA = dcplx{P.qA[2 * s], P.qA[2 * s + 1]};
+      w.qB = dcplx{P.qB[2 * s], P.qB[2 * s + 1]};
+      w.zA = P.zA[s];
+      w.zB = P.zB[s];
+      for (int d = 0; d < 3; ++d) {
+        w.A[d] = dcplx{P.A[6 * s + 2 * d], P.A[6 * s + 2 * d + 1]};
+        w.B[d] = dcplx{P.B[6 * s + 2 * d], P.B[6 * s + 2 * d + 1]};
+      }
+    }
+  }
+  return LFASM_OK;
+}
+
+int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_parts,
+                       const void *d_u, const void *d_lambda, void *d_grad) {
+  if (!h || !d_u || !d_lambda || !d_grad || n_parts < 0 || (n_parts > 0 && !parts))
+    return fail(LFASM_ERR_ARG, "bad gradient arguments");
+  g_err.clear();
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  std::vector<SlabWaveD> waves;
+  int n_slab = 1;
+  // the design elements are the non-PML ones; their slabs must be tabulated
+  int rc = upload_waves(parts, n_parts, h->max_bulk_slab, waves, n_slab);
+  if (rc) return rc;
+  SlabWaveD *dw = nullptr;
+  LF_CUDA(upload(dw, waves.data(), waves.size()));
+  LF_CUDA(cudaMemsetAsync(d_grad, 0, (size_t)h->ne * sizeof(dcplx), h->stream));
+  if (h->n_bulk) {
+    const int wpb = 4;
+    k_eps_grad<<<(h->n_bulk + wpb - 1) / wpb, wpb * 32, 0, h->stream>>>(
+        h->n_bulk, h->bulk_list, h->nd, h->p, h->rm.view(), h->J, h->Jinv, h->detJ, h->v0,
+        h->dof, h->sign, h->fopack, h->pml, h->slab_of, dw, n_slab, n_parts,
+        (const dcplx *)d_u, (const dcplx *)d_lambda, (dcplx *)d_grad);
+    LF_LAUNCHED();
+  }
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  cudaFree(dw);
   return sync_if(h);
 }
 

@@ -906,4 +906,115 @@ __global__ void k_rhs_gather(int n, const int *__restrict__ ea_ptr, const int *_
   }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint contraction for per-element permittivity (one warp per element).
+//
+// For l(u) = c^T u with A(eps) u = b(eps) and A^T lambda = c:
+//   dl/deps_e = lambda^T (db/deps_e - dA/deps_e u)
+//             = k0^2 sum_q w_q detJ [ sum_i Lam_i (lt . v_i)(ut . v_i)
+//                                     + src_e sum_i (lt . v_i) Ehat_i(z_q) ]
+// with dA_e/deps_e = -k0^2 M_e^Lambda (the mass integrator,
+// problem_common.inc:123-148), db_e/deps_e = k0^2 int v . Ehat
+// (ScatterSource, problem_common.inc:238-266), Lam = (s, s, 1/s), v the
+// physical shapes and lt, ut the element-local coefficients of lambda and u
+// (signs and the face transform applied: local = M (sign * global)).
+// ---------------------------------------------------------------------------
+__global__ void k_eps_grad(int nsel, const int *__restrict__ list, int nd, int p, Rule rm,
+                           const double *__restrict__ J9, const double *__restrict__ Ji9,
+                           const double *__restrict__ detJ, const double *__restrict__ v0,
+                           const int *__restrict__ dof, const double *__restrict__ sign,
+                           const unsigned *__restrict__ fopack, PmlParams pml,
+                           const int *__restrict__ slab_of, const SlabWaveD *__restrict__ waves,
+                           int n_slab, int n_parts, const dcplx *__restrict__ u,
+                           const dcplx *__restrict__ lam, dcplx *__restrict__ grad) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= nsel) return;
+  const int e = list[i];
+  double J[9], Ji[9];
+  for (int t = 0; t < 9; ++t) { J[t] = J9[(size_t)e * 9 + t]; Ji[t] = Ji9[(size_t)e * 9 + t]; }
+  const double det = detJ[e];
+  const double z0 = v0[(size_t)e * 3 + 2];
+  const unsigned fp = fopack ? fopack[e] : 0u;
+  // local coefficients for k = lane and k = lane + 32
+  dcplx lt[2], ut[2];
+  for (int hh = 0; hh < 2; ++hh) {
+    const int k = lane + 32 * hh;
+    dcplx lg = mk(0, 0), ug = mk(0, 0);
+    if (k < nd) {
+      const double sg = sign[(size_t)e * nd + k];
+      const int d = dof[(size_t)e * nd + k];
+      lg = cscale(sg, lam[d]);
+      ug = cscale(sg, u[d]);
+    }
+    // face pairs: local = M global, M[r][c] = T[2c + r] (column-major)
+    const double olr = __shfl_xor_sync(0xffffffffu, lg.re, 1);
+    const double oli = __shfl_xor_sync(0xffffffffu, lg.im, 1);
+    const double our = __shfl_xor_sync(0xffffffffu, ug.re, 1);
+    const double oui = __shfl_xor_sync(0xffffffffu, ug.im, 1);
+    const int f = (p >= 2 && k < nd) ? face_of(k & ~1, p) : -1;
+    if (f >= 0) {
+      const double *T = c_tinv + 4 * ((fp >> (8 * f)) & 0xffu);
+      const int r = k & 1;
+      const double own = T[2 * r + r], oth = T[2 * (1 - r) + r];
+      lg = mk(own * lg.re + oth * olr, own * lg.im + oth * oli);
+      ug = mk(own * ug.re + oth * our, own * ug.im + oth * oui);
+    }
+    lt[hh] = lg;
+    ut[hh] = ug;
+  }
+  const int slab = slab_of[e];
+  double gr = 0.0, gi = 0.0;
+  for (int q = 0; q < rm.nq; ++q) {
+    dcplx Lv[3] = {mk(0, 0), mk(0, 0), mk(0, 0)}, Uv[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+    for (int hh = 0; hh < 2; ++hh) {
+      const int k = lane + 32 * hh;
+      if (k >= nd) continue;
+      const double *rv = rm.v + ((size_t)q * nd + k) * 3;
+      for (int d = 0; d < 3; ++d) {
+        const double pv = rv[0] * Ji[0 * 3 + d] + rv[1] * Ji[1 * 3 + d] + rv[2] * Ji[2 * 3 + d];
+        Lv[d] = cadd(Lv[d], cscale(pv, lt[hh]));
+        Uv[d] = cadd(Uv[d], cscale(pv, ut[hh]));
+      }
+    }
+    for (int o = 16; o; o >>= 1)
+      for (int d = 0; d < 3; ++d) {
+        Lv[d].re += __shfl_xor_sync(0xffffffffu, Lv[d].re, o);
+        Lv[d].im += __shfl_xor_sync(0xffffffffu, Lv[d].im, o);
+        Uv[d].re += __shfl_xor_sync(0xffffffffu, Uv[d].re, o);
+        Uv[d].im += __shfl_xor_sync(0xffffffffu, Uv[d].im, o);
+      }
+    if (lane == 0) {
+      const double *xi = rm.ip + q * 3;
+      const double z = z0 + J[6] * xi[0] + J[7] * xi[1] + J[8] * xi[2];
+      const dcplx s = pml_s(pml, z);
+      const dcplx Lam[3] = {s, s, cinv(s)};
+      dcplx acc = mk(0, 0);
+      for (int d = 0; d < 3; ++d) acc = cadd(acc, cmul(Lam[d], cmul(Lv[d], Uv[d])));
+      if (slab >= 0 && n_parts > 0) {
+        dcplx ev[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+        for (int pi = 0; pi < n_parts; ++pi) {
+          const SlabWaveD &sw = waves[(size_t)pi * n_slab + slab];
+          const double da = z - sw.zA, db = z - sw.zB;
+          const double ma = exp(-sw.qA.im * da), mb = exp(-sw.qB.im * db);
+          double sa, ca, sb, cb;
+          sincos(sw.qA.re * da, &sa, &ca);
+          sincos(sw.qB.re * db, &sb, &cb);
+          const dcplx up = mk(ma * ca, ma * sa), dn = mk(mb * cb, mb * sb);
+          for (int d = 0; d < 3; ++d)
+            ev[d] = cadd(ev[d], cadd(cmul(sw.A[d], up), cmul(sw.B[d], dn)));
+        }
+        for (int d = 0; d < 3; ++d) acc = cadd(acc, cmul(Lv[d], ev[d]));
+      }
+      const double w = rm.w[q] * det;
+      gr += w * acc.re;
+      gi += w * acc.im;
+    }
+  }
+  if (lane == 0) {
+    const double k2 = pml.k0 * pml.k0;
+    grad[e] = mk(k2 * gr, k2 * gi);
+  }
+}
+
 }  // namespace lfasm_dev

@@ -121,3 +121,15 @@ def test_difference_layer_gpu(p, h, tol, pol):
     ok, rel = g.ResidualDevice(ud.data_ptr(), bd.data_ptr())
     assert ok and rel < 1e-10
     assert fem_eval.field_error(ad, u, exact, parts) < tol
+
+
+def test_plane_functional_is_the_plane_mean():
+    from lithofem_b200 import adjoint
+    st, ad, pr, parts, exact = fem_eval.difference_layer(2, 3.0)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal(ad.height) + 1j * rng.standard_normal(ad.height)
+    c = adjoint.plane_functional(ad, z=30.0, lx=fem_eval.L, ly=fem_eval.L, comp=1, nx=4, ny=4)
+    xs = (np.arange(4) + 0.5) * fem_eval.L / 4
+    X = np.array([[x, y, 30.0] for y in xs for x in xs])
+    direct = fem_eval.eval_field(ad, u, X)[:, 1].mean()
+    assert abs(c @ u - direct) < 1e-12 * abs(direct)
