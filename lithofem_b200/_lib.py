@@ -64,6 +64,9 @@ def lib() -> ct.CDLL:
                                                   ct.c_void_p]),
         "lfasm_eps_gradient": (ct.c_int, [H, ct.POINTER(IncidentPartC), ct.c_int, ct.c_void_p,
                                           ct.c_void_p, ct.c_void_p]),
+        "lfasm_autotune": (ct.c_int, [H]),
+        "lfasm_set_bulk_variant": (ct.c_int, [H, ct.c_int]),
+        "lfasm_get_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
     }
     for name, (res, args) in sig.items():

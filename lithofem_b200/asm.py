@@ -94,6 +94,19 @@ class AsmGpu:
         _lib.check(_lib.lib().lfasm_stage_times(self._h, out))
         return [float(x) for x in out]
 
+    def Autotune(self) -> bool:
+        return self._ok(_lib.lib().lfasm_autotune(self._h))
+
+    def SetBulkVariant(self, variant: int) -> bool:
+        """0: SIMT bulk-element kernel, 1: FP64 tensor-core (DMMA) variant."""
+        return self._ok(_lib.lib().lfasm_set_bulk_variant(self._h, int(variant)))
+
+    def Tuning(self) -> tuple[int, list[float]]:
+        v = ct.c_int()
+        ms = (ct.c_float * 2)()
+        _lib.check(_lib.lib().lfasm_get_tuning(self._h, ct.byref(v), ms))
+        return v.value, [float(x) for x in ms]
+
     def PathCounts(self) -> tuple[int, int]:
         a, b = ct.c_int(), ct.c_int()
         _lib.check(_lib.lib().lfasm_path_counts(self._h, ct.byref(a), ct.byref(b)))

@@ -101,6 +101,12 @@ struct lfasm_handle {
   int n_bulk = 0, n_pml = 0;
   double *S = nullptr;
   double *rec = nullptr;
+  // tensor-core bulk variant and the autotuned choice
+  double *S_mma = nullptr, *rec_mma = nullptr;
+  int bulk_variant = 0;      // 0: k_bulk (SIMT), 1: k_bulk_mma (DMMA)
+  int tuned = 0;             // autotune done
+  int forced = 0;            // variant fixed by lfasm_set_bulk_variant
+  float tune_ms[2] = {0.f, 0.f};
   dcplx *Ae = nullptr;
   // RHS data
   int *slab_of = nullptr;
@@ -199,6 +205,65 @@ void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
         }
       }
     }
+}
+
+// B operand of the tensor-core bulk variant (k_bulk_mma): the same
+// quadrature sums, term-major [BK][ntiles*8], entries in pair-block order
+// n = 4 (I*H + J) + 2a + b for entry (2I+a, 2J+b), H = ndp/2; terms 0..5 Scc,
+// 6..11 Svv (symmetric pairs), 12..20 Rvc_jj', 21..29 Rcv_jj'.
+int bulk_tiles(int ndp) { const int H = ndp / 2; return (4 * H * H + 7) / 8; }
+
+void build_S_mma(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
+  const int nd = ad->nd;
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  const lfasm_ref_rule &rc = ad->rule_cc, &rm = ad->rule_mass;
+  std::vector<double> Rcc((size_t)9 * nd * nd, 0.0), Rvv(Rcc.size(), 0.0), Rvc(Rcc.size(), 0.0),
+      Rcv(Rcc.size(), 0.0);
+  auto at = [&](std::vector<double> &T, int j, int k, int l) -> double & {
+    return T[((size_t)j * nd + k) * nd + l];
+  };
+  for (int k = 0; k < nd; ++k)
+    for (int l = 0; l < nd; ++l) {
+      for (int q = 0; q < rc.nq; ++q) {
+        const double *ck = rc.curl + ((size_t)q * nd + k) * 3;
+        const double *cl = rc.curl + ((size_t)q * nd + l) * 3;
+        for (int j = 0; j < 3; ++j)
+          for (int jj = 0; jj < 3; ++jj) at(Rcc, j * 3 + jj, k, l) += rc.w[q] * ck[j] * cl[jj];
+      }
+      for (int q = 0; q < rm.nq; ++q) {
+        const double *vk = rm.vshape + ((size_t)q * nd + k) * 3;
+        const double *vl = rm.vshape + ((size_t)q * nd + l) * 3;
+        const double *ck = rm.curl + ((size_t)q * nd + k) * 3;
+        const double *cl = rm.curl + ((size_t)q * nd + l) * 3;
+        for (int j = 0; j < 3; ++j)
+          for (int jj = 0; jj < 3; ++jj) {
+            at(Rvv, j * 3 + jj, k, l) += rm.w[q] * vk[j] * vl[jj];
+            at(Rvc, j * 3 + jj, k, l) += rm.w[q] * vk[j] * cl[jj];
+            at(Rcv, j * 3 + jj, k, l) += rm.w[q] * ck[j] * vl[jj];
+          }
+      }
+    }
+  const int H = ndp / 2, ntiles = bulk_tiles(ndp), N = ntiles * 8;
+  S.assign((size_t)BK * N, 0.0);
+  for (int I = 0; I < H; ++I)
+    for (int Jp = 0; Jp < H; ++Jp)
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          const int k = 2 * I + a, l = 2 * Jp + b;
+          if (k >= nd || l >= nd) continue;
+          const size_t n = (size_t)4 * (I * H + Jp) + 2 * a + b;
+          for (int t = 0; t < 6; ++t) {
+            const int x = pa[t], y = pb[t];
+            S[(size_t)t * N + n] = x == y ? at(Rcc, x * 3 + x, k, l)
+                                          : at(Rcc, x * 3 + y, k, l) + at(Rcc, y * 3 + x, k, l);
+            S[(size_t)(6 + t) * N + n] = x == y ? at(Rvv, x * 3 + x, k, l)
+                                                : at(Rvv, x * 3 + y, k, l) + at(Rvv, y * 3 + x, k, l);
+          }
+          for (int j = 0; j < 9; ++j) {
+            S[(size_t)(12 + j) * N + n] = at(Rvc, j, k, l);
+            S[(size_t)(21 + j) * N + n] = at(Rcv, j, k, l);
+          }
+        }
 }
 
 // 2x2 blocks relating element-local face DOF pairs to the global pairs for
@@ -405,6 +470,10 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   std::vector<double> S;
   build_S(ad, h->ndp, S);
   LF_CUDA_H(upload(h->S, S.data(), S.size()));
+  build_S_mma(ad, h->ndp, S);
+  LF_CUDA_H(upload(h->S_mma, S.data(), S.size()));
+  if (h->n_bulk)
+    LF_CUDA_H(cudaMalloc(&h->rec_mma, (size_t)h->n_bulk * BREC * sizeof(double)));
 
   // RHS source elements: frustum regions (delta = region eps - eps_bg) or,
   // with per-element eps, every non-PML element whose eps differs from its
@@ -527,7 +596,7 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     LF_CUDA(cudaStreamWaitEvent(h->side, h->fork, 0));
   }
   const int rs = mode ? h->ndp : h->nd;
-  if (h->n_bulk) {
+  if (h->n_bulk && h->bulk_variant == 0) {
     const int nb = h->n_bulk;
     k_prep_bulk<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
                                                          h->detJ, h->attr, h->eps_tab,
@@ -535,8 +604,6 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     LF_LAUNCHED();
     const int nthr = bulk_threads(h->ndp);
     const int ytiles = (nthr + BULK_THREADS - 1) / BULK_THREADS;
-    // about two waves of resident blocks; each block keeps its S-table
-    // values in registers across its chunk of elements
     const long long want = (long long)h->sm_count * 8;
     int chunk = (int)std::max<long long>(16, ((long long)nb * ytiles + want - 1) / want);
     chunk = (chunk + BULK_EB - 1) / BULK_EB * BULK_EB;
@@ -549,6 +616,27 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     if (cross) { if (mode) LF_BULK(true, 1); else LF_BULK(true, 0); }
     else { if (mode) LF_BULK(false, 1); else LF_BULK(false, 0); }
 #undef LF_BULK
+    LF_LAUNCHED();
+  } else if (h->n_bulk) {
+    const int nb = h->n_bulk;
+    k_prep_bulk_mma<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
+                                                             h->detJ, h->attr, h->eps_tab,
+                                                             h->elem_eps, h->pml, mask,
+                                                             h->rec_mma);
+    LF_LAUNCHED();
+    const int ntiles = bulk_tiles(h->ndp);
+    const int ytiles = (ntiles + BULK_WARPS * BULK_T - 1) / (BULK_WARPS * BULK_T);
+    const int nbat = (nb + 7) / 8;
+    const long long want = (long long)h->sm_count * 8;
+    const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
+    dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
+#define LF_BULKM(C, M)                                                            \
+  k_bulk_mma<C, M><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                      \
+      nb, h->bulk_list, h->rec_mma, h->S_mma, ntiles, h->nd, h->ndp, h->p, bchunk, \
+      te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
+    if (cross) { if (mode) LF_BULKM(true, 1); else LF_BULKM(true, 0); }
+    else { if (mode) LF_BULKM(false, 1); else LF_BULKM(false, 0); }
+#undef LF_BULKM
     LF_LAUNCHED();
   }
   if (prof) LF_CUDA(cudaEventRecord(h->ev[1], h->stream));
@@ -750,10 +838,65 @@ int lfasm_scatter_eliminate(lfasm_handle *h, int eliminate) {
   return sync_if(h);
 }
 
+// Autotuner: times each bulk-element variant on this mesh (two launches
+// each, the second timed with CUDA events) and keeps the faster one.
+int lfasm_autotune(lfasm_handle *h) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  LF_CUDA(cudaSetDevice(h->dev));
+  const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
+  cudaEvent_t a, b;
+  LF_CUDA(cudaEventCreate(&a));
+  LF_CUDA(cudaEventCreate(&b));
+  const int keep_n_pml = h->n_pml;
+  h->n_pml = 0;  // time the bulk path alone
+  int rc = LFASM_OK;
+  for (int v = 0; v < 2 && !rc; ++v) {
+    h->bulk_variant = v;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+      LF_CUDA(cudaEventRecord(a, h->stream));
+      rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, 1);
+      LF_CUDA(cudaEventRecord(b, h->stream));
+    }
+    if (!rc) {
+      LF_CUDA(cudaEventSynchronize(b));
+      LF_CUDA(cudaEventElapsedTime(&h->tune_ms[v], a, b));
+    }
+  }
+  h->n_pml = keep_n_pml;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  h->bulk_variant = h->tune_ms[1] < h->tune_ms[0] ? 1 : 0;
+  h->tuned = 1;
+  h->locals_valid = 0;
+  return sync_if(h);
+}
+
+int lfasm_set_bulk_variant(lfasm_handle *h, int variant) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (variant < 0 || variant > 1) return fail(LFASM_ERR_ARG, "bulk variant must be 0 or 1");
+  h->bulk_variant = variant;
+  h->forced = 1;
+  h->tuned = 1;
+  return LFASM_OK;
+}
+
+int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms2) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (bulk_variant) *bulk_variant = h->bulk_variant;
+  if (ms2) { ms2[0] = h->tune_ms[0]; ms2[1] = h->tune_ms[1]; }
+  return LFASM_OK;
+}
+
 int lfasm_assemble(lfasm_handle *h, int eliminate) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   g_err.clear();
   if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
+  if (!h->tuned) {
+    int rt = lfasm_autotune(h);
+    if (rt) return rt;
+  }
   const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
   int rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, eliminate ? 1 : 0);
   if (rc) return rc;
@@ -1061,7 +1204,7 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
   for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
-  dfree(h->S); dfree(h->rec); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
+  dfree(h->S); dfree(h->rec); dfree(h->S_mma); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
   dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->off); dfree(h->partials);
   dfree(h->red);

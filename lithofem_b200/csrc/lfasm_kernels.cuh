@@ -289,6 +289,192 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 }
 
 // ---------------------------------------------------------------------------
+// Bulk elements as a tensor-core GEMM (alternative to k_bulk, chosen by the
+// autotuner).  A_e = sum_t G_e[t] S_t written as C (8 elements x 8 entries)
+// = A (8 x 32 terms) B (32 x 8) per m8n8k4 DMMA tile: A = the element
+// coefficient rows (a real row: terms 0..11, an imaginary row: 6..29), B = S
+// in pair-block-major entry order n = 4 pb + 2a + b for entry (2I+a, 2J+b).
+// Terms: 0..5 curl-curl and 6..11 mass+KLK at the symmetric pairs, 12..20
+// MixedVectorCurl (Jinv K J), 21..29 MixedVectorWeakCurl (J^T K Jinv^T).
+// Each warp keeps its B fragments and its per-tile entry indices in
+// registers; the face table is read from shared memory (lanes hold different
+// elements).
+// ---------------------------------------------------------------------------
+constexpr int BK = 32;          // coefficient terms (padded)
+constexpr int BREC = 2 * BK;    // doubles per element record: real row, imaginary row
+constexpr int BULK_T = 4;       // N tiles (8 entries) per warp
+constexpr int BULK_WARPS = 4;
+
+__global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
+                            const double *__restrict__ J9, const double *__restrict__ Ji9,
+                            const double *__restrict__ detJ, const int *__restrict__ attr,
+                            const dcplx *__restrict__ eps_tab,
+                            const dcplx *__restrict__ elem_eps, PmlParams pml,
+                            int mask, double *__restrict__ rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const int e = list[i];
+  double J[9], Ji[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    J[t] = J9[(size_t)e * 9 + t];
+    Ji[t] = Ji9[(size_t)e * 9 + t];
+  }
+  const double det = detJ[e];
+  const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+  double *re = rec + (size_t)i * BREC, *im = re + BK;
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  const bool cc = mask & 1, ms = mask & 2, c0 = mask & 4, c1 = mask & 8, kl = mask & 16;
+  const double kx = pml.kx, ky = pml.ky, k2 = pml.k0 * pml.k0;
+  // K = [[0,0,ky],[0,0,-kx],[-ky,kx,0]] (fill_K, problem_common.inc:150-158)
+  const double K[9] = {0.0, 0.0, ky, 0.0, 0.0, -kx, -ky, kx, 0.0};
+  // -K K (real symmetric), the KLK tensor where Lambda = I
+  const double mKK[9] = {ky * ky, -kx * ky, 0.0, -kx * ky, kx * kx, 0.0, 0.0, 0.0,
+                         kx * kx + ky * ky};
+  const double me_re = -k2 * eps.re, me_im = -k2 * eps.im;
+  for (int t = 0; t < BK; ++t) { re[t] = 0.0; im[t] = 0.0; }
+  for (int t = 0; t < 6; ++t) {
+    const int a = pa[t], b = pb[t];
+    if (cc) re[t] = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
+    const double jj = Ji[a * 3 + 0] * Ji[b * 3 + 0] + Ji[a * 3 + 1] * Ji[b * 3 + 1] +
+                      Ji[a * 3 + 2] * Ji[b * 3 + 2];
+    double vr = 0.0, vi = 0.0;
+    if (ms) { vr += me_re * jj; vi += me_im * jj; }
+    if (kl) {
+      double s = 0.0;
+      for (int rr = 0; rr < 3; ++rr)
+        for (int c2 = 0; c2 < 3; ++c2) s += Ji[a * 3 + rr] * mKK[rr * 3 + c2] * Ji[b * 3 + c2];
+      vr += s;
+    }
+    re[6 + t] = det * vr;
+    im[6 + t] = det * vi;
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double gvc = 0.0, gcv = 0.0;
+      for (int rr = 0; rr < 3; ++rr)
+        for (int c2 = 0; c2 < 3; ++c2) {
+          const double k = K[rr * 3 + c2];
+          if (k == 0.0) continue;
+          gvc += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
+          gcv += J[rr * 3 + a] * k * Ji[b * 3 + c2];
+        }
+      if (c0) im[12 + a * 3 + b] = gvc;
+      if (c1) im[21 + a * 3 + b] = gcv;
+    }
+}
+
+// ncol_tiles: total N tiles (entries / 8, rounded up); nbatch: element batches
+// of 8.  Block: BULK_WARPS warps, N tiles [blockIdx.y*BULK_WARPS*BULK_T, ...).
+template <bool CROSS, int MODE>
+__global__ void __launch_bounds__(BULK_WARPS * 32)
+k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
+           const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
+           int eliminate, int rs, const unsigned *__restrict__ fopack,
+           const unsigned long long *__restrict__ signmask,
+           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
+  __shared__ double sA[8 * BREC];
+  __shared__ double sT[24];
+  __shared__ int se[8];
+  __shared__ unsigned sfo[8];
+  __shared__ unsigned long long ssm[8], sem[8];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int H = ndp >> 1, npb = H * H;
+  if (tid < 24) sT[tid] = c_tinv[tid];
+  constexpr int KS = BK / 4;
+  double bf[BULK_T][KS];
+  // per-tile constants (independent of the element): entries
+  // n = tile*8 + 2*t4 + {0,1} -> pair block pb = tile*2 + (t4 >> 1),
+  // row 2I + a (a = t4 & 1), columns 2J, 2J+1
+  int rowv[BULK_T], colv[BULK_T], frv[BULK_T], fcv[BULK_T], okv[BULK_T];
+  const int tile0 = (blockIdx.y * BULK_WARPS + w) * BULK_T;
+#pragma unroll
+  for (int j = 0; j < BULK_T; ++j) {
+    const int tile = tile0 + j;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks)
+      bf[j][ks] = tile < ntiles ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
+    const int pb = tile * 2 + (t4 >> 1);
+    const bool ok = tile < ntiles && pb < npb;
+    const int I = ok ? pb / H : 0, Jp = ok ? pb - I * H : 0;
+    rowv[j] = 2 * I + (t4 & 1);
+    colv[j] = 2 * Jp;
+    okv[j] = ok && rowv[j] < nd && colv[j] < nd;
+    frv[j] = (te && p >= 2) ? face_of(2 * I, p) : -1;
+    fcv[j] = (te && p >= 2) ? face_of(2 * Jp, p) : -1;
+  }
+  const int a = t4 & 1;
+  const int nbat = (nb + 7) / 8;
+  const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
+  for (int bt = b0; bt < b1; ++bt) {
+    const int ebase = bt * 8;
+    const int nel = min(8, nb - ebase);
+    __syncthreads();
+    for (int j = tid; j < 8 * BREC; j += BULK_WARPS * 32)
+      sA[j] = (j / BREC) < nel ? rec[(size_t)ebase * BREC + j] : 0.0;
+    if (tid < 8) {
+      const int e = tid < nel ? list[ebase + tid] : -1;
+      se[tid] = e;
+      sfo[tid] = e >= 0 ? fopack[e] : 0u;
+      ssm[tid] = (MODE == 1 && e >= 0) ? signmask[e] : 0ull;
+      sem[tid] = (MODE == 1 && e >= 0 && eliminate) ? essmask[e] : 0ull;
+    }
+    __syncthreads();
+    double ar[3], ai[KS];
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * BREC + ks * 4 + t4];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) ai[ks] = sA[g * BREC + BK + ks * 4 + t4];
+    const int e = se[g];
+    const unsigned fp = sfo[g];
+    const unsigned long long sm = ssm[g], em = sem[g];
+    dcplx *base = e >= 0 ? Ae + (size_t)e * nd * rs : Ae;
+#pragma unroll
+    for (int j = 0; j < BULK_T; ++j) {
+      double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 3; ++ks) dmma(cr0, cr1, ar[ks], bf[j][ks]);
+#pragma unroll
+      for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci0, ci1, ai[ks], bf[j][ks]);
+      if (fcv[j] >= 0) {  // columns: the pair is thread-local
+        const double *T = sT + 4 * ((fp >> (8 * fcv[j])) & 0xffu);
+        const double n0 = T[0] * cr0 + T[1] * cr1, n1 = T[2] * cr0 + T[3] * cr1;
+        const double m0 = T[0] * ci0 + T[1] * ci1, m1 = T[2] * ci0 + T[3] * ci1;
+        cr0 = n0; cr1 = n1; ci0 = m0; ci1 = m1;
+      }
+      if (te && p >= 2) {  // rows: partner row in lane t4 ^ 1
+        const double qr0 = __shfl_xor_sync(0xffffffffu, cr0, 1);
+        const double qr1 = __shfl_xor_sync(0xffffffffu, cr1, 1);
+        const double qi0 = __shfl_xor_sync(0xffffffffu, ci0, 1);
+        const double qi1 = __shfl_xor_sync(0xffffffffu, ci1, 1);
+        if (frv[j] >= 0) {
+          const double *T = sT + 4 * ((fp >> (8 * frv[j])) & 0xffu);
+          const double own = T[2 * a + a], oth = T[2 * a + 1 - a];
+          cr0 = own * cr0 + oth * qr0; cr1 = own * cr1 + oth * qr1;
+          ci0 = own * ci0 + oth * qi0; ci1 = own * ci1 + oth * qi1;
+        }
+      }
+      if (!okv[j] || e < 0) continue;
+      const int row = rowv[j], col = colv[j];
+      if (MODE == 1) {
+        const unsigned long long rbit = (sm >> row) & 1ull, cb = sm >> col;
+        const double s0 = ((rbit ^ cb) & 1ull) ? -1.0 : 1.0;
+        const double s1 = ((rbit ^ (cb >> 1)) & 1ull) ? -1.0 : 1.0;
+        cr0 *= s0; ci0 *= s0; cr1 *= s1; ci1 *= s1;
+        const unsigned long long eb = em >> col;
+        const bool er = (em >> row) & 1ull;
+        if (er || (eb & 1ull)) { cr0 = 0.0; ci0 = 0.0; }
+        if (er || (eb & 2ull)) { cr1 = 0.0; ci1 = 0.0; }
+      }
+      dcplx *dst = base + (size_t)row * rs + col;
+      dst[0] = mk(cr0, ci0);
+      if (col + 1 < nd) dst[1] = mk(cr1, ci1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // PML element kernel on FP64 tensor cores (mma.sync m8n8k4 .f64, DMMA).
 //
 // Per element: A_e = sum_r X[r]^T Y[r] over the staged rows r (3 curl rows

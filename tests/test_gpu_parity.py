@@ -222,3 +222,32 @@ def test_against_reference_cuda_kernels(kcase):
     loc_ref, _ = rc.gpu_local(CURLCURL, mm, True)
     assert g.ComputeLocal(CURLCURL, mm, True)
     assert rel(g.DownloadLocal(), loc_ref) < TOL
+
+
+@pytest.mark.parametrize("kcase", [("grating", 3, 6.0), ("hole", 2, 0.0), ("hole", 1, 6.0), ("slab", 3, 6.0)], ids=ids)
+@pytest.mark.parametrize("variant", [0, 1], ids=["simt", "dmma"])
+def test_bulk_variants(kcase, variant):
+    """Both bulk-element kernels (the autotuner's candidates) match the oracle."""
+    c = case(*kcase) if kcase[0] != "slab" else configs.small_case("slab", 3, 6.0, seed=13, h=3.2)
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(c.ad, 0) and g.SetBulkVariant(variant)
+    mm = MASS | ((CROSS0 | CROSS1 | KLK) if c.prob.has_kpar else 0)
+    for te in (False, True):
+        assert g.ComputeLocal(CURLCURL, mm, te)
+        assert rel(g.DownloadLocal(), oracle.local(c.ad, c.prob, CURLCURL, mm, te)) < TOL
+    if c.prob.has_kpar:
+        for m in (CROSS0, CROSS1, KLK):
+            assert g.ComputeLocal(0, m, False)
+            assert rel(g.DownloadLocal(), oracle.local(c.ad, c.prob, 0, m, False)) < TOL
+    assert g.BuildGlobal(c.ad.ess) and g.Assemble(True)
+    I, J = oracle.csr(c.ad)
+    assert rel(g.DownloadValues(), oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, True)) < TOL
+    assert g.Tuning()[0] == variant
+
+
+def test_autotuner_picks_a_variant():
+    c = case("grating", 2, 6.0)
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
+    v, ms = g.Tuning()
+    assert v in (0, 1) and ms[0] > 0 and ms[1] > 0 and ms[v] == min(ms)
