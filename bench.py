@@ -297,6 +297,8 @@ def run_ours(a, rank, world, local, dist, torch):
     assert g.BuildGlobal(ad.ess)
     case.nnz = g.nnz()
     nb, npml = g.PathCounts()
+    assert g.Autotune()
+    tuning = g.Tuning()
     # warm-up
     for _ in range(a.warmup):
         assert g.Assemble(True)
@@ -409,7 +411,9 @@ def run_ours(a, rank, world, local, dist, torch):
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64}
+            "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
+            "tuning": {"bulk_variant": ["k_bulk (SIMT)", "k_bulk_mma (DMMA)"][tuning[0]],
+                       "bulk_ms": tuning[1]}}
     print(json.dumps(line), flush=True)
     g.Release()
     if dist is not None:

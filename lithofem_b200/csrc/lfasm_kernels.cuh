@@ -157,7 +157,7 @@ __global__ void k_prep_bulk(int nb, const int *__restrict__ list,
 constexpr int BULK_EB = 8;
 
 template <bool CROSS, int MODE>
-__global__ void __launch_bounds__(BULK_THREADS)
+__global__ void __launch_bounds__(BULK_THREADS, 3)
 k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
        const double *__restrict__ S, int nthr, int nd, int ndp, int p, int chunk, int te,
        int eliminate, int rs, int c0, int c1, const unsigned *__restrict__ fopack,
@@ -166,6 +166,8 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   constexpr int NV = CROSS ? 60 : 24;
   __shared__ double sg[BULK_EB * REC];
   __shared__ int se[BULK_EB];
+  __shared__ unsigned sfo[BULK_EB];
+  __shared__ unsigned long long ssm[BULK_EB], sem[BULK_EB];
   const int tid = threadIdx.x;
   const int f = blockIdx.y * BULK_THREADS + tid;
   const bool valid = f < nthr;
@@ -190,7 +192,13 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
     const int nbat = min(BULK_EB, i1 - ib);
     __syncthreads();
     for (int j = tid; j < nbat * REC; j += BULK_THREADS) sg[j] = rec[(size_t)ib * REC + j];
-    if (tid < nbat) se[tid] = list[ib + tid];
+    if (tid < nbat) {
+      const int e = list[ib + tid];
+      se[tid] = e;
+      sfo[tid] = fopack[e];
+      ssm[tid] = MODE == 1 ? signmask[e] : 0ull;
+      sem[tid] = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+    }
     __syncthreads();
     for (int b = 0; b < nbat; ++b) {
       const double *g = sg + b * REC;
@@ -229,7 +237,7 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
       }
       const int e = se[b];
       if (te && p >= 2) {
-        const unsigned fp = fopack[e];
+        const unsigned fp = sfo[b];
         // primary: columns (partner lane holds column l^1), then rows
         const double qpr0 = __shfl_xor_sync(0xffffffffu, pr0, 1);
         const double qpi0 = __shfl_xor_sync(0xffffffffu, pi0, 1);
@@ -262,14 +270,14 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
         }
       }
       if (MODE == 1 && valid) {
-        const unsigned long long sm = signmask[e];
+        const unsigned long long sm = ssm[b];
         const double sl = ((sm >> l) & 1ull) ? -1.0 : 1.0;
         const double sa = (((sm >> r0) & 1ull) ? -1.0 : 1.0) * sl;
         const double sb = (((sm >> r1) & 1ull) ? -1.0 : 1.0) * sl;
         pr0 *= sa; pi0 *= sa; pr1 *= sb; pi1 *= sb;
         mr0 *= sa; mi0 *= sa; mr1 *= sb; mi1 *= sb;
         if (eliminate) {
-          const unsigned long long em = essmask[e];
+          const unsigned long long em = sem[b];
           const bool el = (em >> l) & 1ull;
           if (el || ((em >> r0) & 1ull)) { pr0 = pi0 = mr0 = mi0 = 0.0; }
           if (el || ((em >> r1) & 1ull)) { pr1 = pi1 = mr1 = mi1 = 0.0; }
