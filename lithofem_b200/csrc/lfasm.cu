@@ -84,7 +84,7 @@ struct lfasm_handle {
   cudaStream_t stream = nullptr;
   int async_mode = 0;
   int ne = 0, nd = 0, p = 0, n = 0, has_kpar = 0;
-  int ndp = 0, ndp4 = 0;
+  int ndp = 0, ndp4 = 0, rs = 0;
   int sm_count = 148;
   long long nnz = 0;
   // element data
@@ -211,7 +211,7 @@ void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
 // quadrature sums, term-major [BK][ntiles*8], entries in pair-block order
 // n = 4 (I*H + J) + 2a + b for entry (2I+a, 2J+b), H = ndp/2; terms 0..5 Scc,
 // 6..11 Svv (symmetric pairs), 12..20 Rvc_jj', 21..29 Rcv_jj'.
-int bulk_tiles(int ndp) { const int H = ndp / 2; return (4 * H * H + 7) / 8; }
+int bulk_tiles(int ndp) { return 2 * (ndp / 2) * ((ndp + 7) / 8); }
 
 void build_S_mma(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
   const int nd = ad->nd;
@@ -243,15 +243,15 @@ void build_S_mma(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
           }
       }
     }
-  const int H = ndp / 2, ntiles = bulk_tiles(ndp), N = ntiles * 8;
+  const int ncb = (ndp + 7) / 8, ntiles = bulk_tiles(ndp), N = ntiles * 8;
   S.assign((size_t)BK * N, 0.0);
-  for (int I = 0; I < H; ++I)
-    for (int Jp = 0; Jp < H; ++Jp)
+  for (int I = 0; I < ndp / 2; ++I)
+    for (int cb = 0; cb < ncb; ++cb)
       for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b) {
-          const int k = 2 * I + a, l = 2 * Jp + b;
+        for (int c = 0; c < 8; ++c) {
+          const int k = 2 * I + a, l = 8 * cb + c;
           if (k >= nd || l >= nd) continue;
-          const size_t n = (size_t)4 * (I * H + Jp) + 2 * a + b;
+          const size_t n = (size_t)(2 * (I * ncb + cb) + a) * 8 + c;
           for (int t = 0; t < 6; ++t) {
             const int x = pa[t], y = pb[t];
             S[(size_t)t * N + n] = x == y ? at(Rcc, x * 3 + x, k, l)
@@ -354,6 +354,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   h->n = ad->height;
   h->has_kpar = (prob->kx != 0.0 || prob->ky != 0.0) ? 1 : 0;
   h->ndp = (nd + 1) & ~1;
+  h->rs = (nd + 7) & ~7;  // fused element-buffer row stride: rows on 128-byte lines
   h->ndp4 = (nd + 3) & ~3;
   if (ad->I || ad->Jcol) {
     if (!ad->I || !ad->Jcol || ad->nnz <= 0) {
@@ -521,7 +522,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   // element buffer: dense nd x nd rows for lfasm_compute_local, padded row
   // stride ndp (even) for the fused path so every row starts on a 32-byte
   // sector and column pairs fill whole sectors
-  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * h->ndp * sizeof(dcplx)));
+  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * h->rs * sizeof(dcplx)));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
   LF_CUDA_H(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   LF_CUDA_H(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
@@ -595,7 +596,7 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     LF_CUDA(cudaEventRecord(h->fork, h->stream));
     LF_CUDA(cudaStreamWaitEvent(h->side, h->fork, 0));
   }
-  const int rs = mode ? h->ndp : h->nd;
+  const int rs = mode ? h->rs : h->nd;
   if (h->n_bulk && h->bulk_variant == 0) {
     const int nb = h->n_bulk;
     k_prep_bulk<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
@@ -626,6 +627,8 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     LF_LAUNCHED();
     const int ntiles = bulk_tiles(h->ndp);
     const int ytiles = (ntiles + BULK_WARPS * BULK_T - 1) / (BULK_WARPS * BULK_T);
+    // k_bulk_mma writes 16-byte-aligned double4 pairs: needs rs even (the
+    // fused layout); the dense ComputeLocal layout uses the SIMT kernel
     const int nbat = (nb + 7) / 8;
     const long long want = (long long)h->sm_count * 8;
     const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
@@ -820,7 +823,7 @@ static int gather(lfasm_handle *h, bool raw, int eliminate) {
   } else {
     LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_gather<false><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
-                                                       h->Ae, h->nd, h->ndp, h->ess, h->sign, h->dof,
+                                                       h->Ae, h->nd, h->rs, h->ess, h->sign, h->dof,
                                                        eliminate, h->max_row, h->vals);
   }
   LF_LAUNCHED();

@@ -372,8 +372,11 @@ __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
     }
 }
 
-// ncol_tiles: total N tiles (entries / 8, rounded up); nbatch: element batches
-// of 8.  Block: BULK_WARPS warps, N tiles [blockIdx.y*BULK_WARPS*BULK_T, ...).
+// Tiles are 8 consecutive columns of one row: tile t = 2 (I * ncb + cb) + a
+// covers entry (2I + a, 8 cb + c), c = 0..7, so a warp's C fragment for one
+// element is one full 128-byte line of the (row-padded) element matrix.  A
+// warp owns BULK_T/2 row-pair blocks (I, cb), i.e. both rows of each pair:
+// the row transform is thread-local, the column pair is thread-local.
 template <bool CROSS, int MODE>
 __global__ void __launch_bounds__(BULK_WARPS * 32)
 k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
@@ -386,33 +389,34 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   __shared__ int se[8];
   __shared__ unsigned sfo[8];
   __shared__ unsigned long long ssm[8], sem[8];
+  constexpr int PB = BULK_T / 2;           // row-pair blocks per warp
+  constexpr int KS = BK / 4;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
-  const int H = ndp >> 1, npb = H * H;
+  const int ncb = (ndp + 7) / 8;           // column blocks of 8
+  const int npb = (ndp / 2) * ncb;         // row-pair blocks
   if (tid < 24) sT[tid] = c_tinv[tid];
-  constexpr int KS = BK / 4;
-  double bf[BULK_T][KS];
-  // per-tile constants (independent of the element): entries
-  // n = tile*8 + 2*t4 + {0,1} -> pair block pb = tile*2 + (t4 >> 1),
-  // row 2I + a (a = t4 & 1), columns 2J, 2J+1
-  int rowv[BULK_T], colv[BULK_T], frv[BULK_T], fcv[BULK_T], okv[BULK_T];
-  const int tile0 = (blockIdx.y * BULK_WARPS + w) * BULK_T;
+  double bf[PB][2][KS];
+  int rowv[PB], colv[PB], frv[PB], fcv[PB], okv[PB];
+  const int pb0 = (blockIdx.y * BULK_WARPS + w) * PB;
 #pragma unroll
-  for (int j = 0; j < BULK_T; ++j) {
-    const int tile = tile0 + j;
+  for (int j = 0; j < PB; ++j) {
+    const int pb = pb0 + j;
+    const bool ok = pb < npb;
 #pragma unroll
-    for (int ks = 0; ks < KS; ++ks)
-      bf[j][ks] = tile < ntiles ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
-    const int pb = tile * 2 + (t4 >> 1);
-    const bool ok = tile < ntiles && pb < npb;
-    const int I = ok ? pb / H : 0, Jp = ok ? pb - I * H : 0;
-    rowv[j] = 2 * I + (t4 & 1);
-    colv[j] = 2 * Jp;
+    for (int a = 0; a < 2; ++a) {
+      const int tile = 2 * pb + a;
+#pragma unroll
+      for (int ks = 0; ks < KS; ++ks)
+        bf[j][a][ks] = ok ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
+    }
+    const int I = ok ? pb / ncb : 0, cb = ok ? pb - I * ncb : 0;
+    rowv[j] = 2 * I;
+    colv[j] = 8 * cb + 2 * t4;
     okv[j] = ok && rowv[j] < nd && colv[j] < nd;
     frv[j] = (te && p >= 2) ? face_of(2 * I, p) : -1;
-    fcv[j] = (te && p >= 2) ? face_of(2 * Jp, p) : -1;
+    fcv[j] = (te && p >= 2) ? face_of(colv[j], p) : -1;
   }
-  const int a = t4 & 1;
   const int nbat = (nb + 7) / 8;
   const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
   for (int bt = b0; bt < b1; ++bt) {
@@ -439,45 +443,59 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
     const unsigned long long sm = ssm[g], em = sem[g];
     dcplx *base = e >= 0 ? Ae + (size_t)e * nd * rs : Ae;
 #pragma unroll
-    for (int j = 0; j < BULK_T; ++j) {
-      double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+    for (int j = 0; j < PB; ++j) {
+      // c[a][i]: row 2I + a, column col + i
+      double cr[2][2], ci[2][2];
 #pragma unroll
-      for (int ks = 0; ks < 3; ++ks) dmma(cr0, cr1, ar[ks], bf[j][ks]);
+      for (int a = 0; a < 2; ++a) {
+        cr[a][0] = cr[a][1] = ci[a][0] = ci[a][1] = 0.0;
 #pragma unroll
-      for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci0, ci1, ai[ks], bf[j][ks]);
-      if (fcv[j] >= 0) {  // columns: the pair is thread-local
-        const double *T = sT + 4 * ((fp >> (8 * fcv[j])) & 0xffu);
-        const double n0 = T[0] * cr0 + T[1] * cr1, n1 = T[2] * cr0 + T[3] * cr1;
-        const double m0 = T[0] * ci0 + T[1] * ci1, m1 = T[2] * ci0 + T[3] * ci1;
-        cr0 = n0; cr1 = n1; ci0 = m0; ci1 = m1;
-      }
-      if (te && p >= 2) {  // rows: partner row in lane t4 ^ 1
-        const double qr0 = __shfl_xor_sync(0xffffffffu, cr0, 1);
-        const double qr1 = __shfl_xor_sync(0xffffffffu, cr1, 1);
-        const double qi0 = __shfl_xor_sync(0xffffffffu, ci0, 1);
-        const double qi1 = __shfl_xor_sync(0xffffffffu, ci1, 1);
-        if (frv[j] >= 0) {
-          const double *T = sT + 4 * ((fp >> (8 * frv[j])) & 0xffu);
-          const double own = T[2 * a + a], oth = T[2 * a + 1 - a];
-          cr0 = own * cr0 + oth * qr0; cr1 = own * cr1 + oth * qr1;
-          ci0 = own * ci0 + oth * qi0; ci1 = own * ci1 + oth * qi1;
-        }
+        for (int ks = 0; ks < 3; ++ks) dmma(cr[a][0], cr[a][1], ar[ks], bf[j][a][ks]);
+#pragma unroll
+        for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
       }
       if (!okv[j] || e < 0) continue;
-      const int row = rowv[j], col = colv[j];
-      if (MODE == 1) {
-        const unsigned long long rbit = (sm >> row) & 1ull, cb = sm >> col;
-        const double s0 = ((rbit ^ cb) & 1ull) ? -1.0 : 1.0;
-        const double s1 = ((rbit ^ (cb >> 1)) & 1ull) ? -1.0 : 1.0;
-        cr0 *= s0; ci0 *= s0; cr1 *= s1; ci1 *= s1;
-        const unsigned long long eb = em >> col;
-        const bool er = (em >> row) & 1ull;
-        if (er || (eb & 1ull)) { cr0 = 0.0; ci0 = 0.0; }
-        if (er || (eb & 2ull)) { cr1 = 0.0; ci1 = 0.0; }
+      if (fcv[j] >= 0) {  // columns: A <- A M
+        const double *T = sT + 4 * ((fp >> (8 * fcv[j])) & 0xffu);
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const double n0 = T[0] * cr[a][0] + T[1] * cr[a][1], n1 = T[2] * cr[a][0] + T[3] * cr[a][1];
+          const double m0 = T[0] * ci[a][0] + T[1] * ci[a][1], m1 = T[2] * ci[a][0] + T[3] * ci[a][1];
+          cr[a][0] = n0; cr[a][1] = n1; ci[a][0] = m0; ci[a][1] = m1;
+        }
       }
-      dcplx *dst = base + (size_t)row * rs + col;
-      dst[0] = mk(cr0, ci0);
-      if (col + 1 < nd) dst[1] = mk(cr1, ci1);
+      if (frv[j] >= 0) {  // rows: A <- M^T A
+        const double *T = sT + 4 * ((fp >> (8 * frv[j])) & 0xffu);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const double n0 = T[0] * cr[0][i] + T[1] * cr[1][i], n1 = T[2] * cr[0][i] + T[3] * cr[1][i];
+          const double m0 = T[0] * ci[0][i] + T[1] * ci[1][i], m1 = T[2] * ci[0][i] + T[3] * ci[1][i];
+          cr[0][i] = n0; cr[1][i] = n1; ci[0][i] = m0; ci[1][i] = m1;
+        }
+      }
+      const int row = rowv[j], col = colv[j];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int r = row + a;
+        if (r >= nd) continue;
+        if (MODE == 1) {
+          const unsigned long long rbit = (sm >> r) & 1ull, cbits = sm >> col;
+          const double s0 = ((rbit ^ cbits) & 1ull) ? -1.0 : 1.0;
+          const double s1 = ((rbit ^ (cbits >> 1)) & 1ull) ? -1.0 : 1.0;
+          cr[a][0] *= s0; ci[a][0] *= s0; cr[a][1] *= s1; ci[a][1] *= s1;
+          const unsigned long long eb = em >> col;
+          const bool er = (em >> r) & 1ull;
+          if (er || (eb & 1ull)) { cr[a][0] = 0.0; ci[a][0] = 0.0; }
+          if (er || (eb & 2ull)) { cr[a][1] = 0.0; ci[a][1] = 0.0; }
+        }
+        dcplx *dst = base + (size_t)r * rs + col;
+        if (col + 1 < nd && (reinterpret_cast<uintptr_t>(dst) & 31u) == 0) {
+          reinterpret_cast<double4 *>(dst)[0] = make_double4(cr[a][0], ci[a][0], cr[a][1], ci[a][1]);
+        } else {
+          dst[0] = mk(cr[a][0], ci[a][0]);
+          if (col + 1 < nd) dst[1] = mk(cr[a][1], ci[a][1]);
+        }
+      }
     }
   }
 }
