@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bulk-variant", type=int, default=-1,
+                    help="force the bulk-element kernel (0 SIMT, 1 DMMA); default: autotune")
     return ap.parse_args()
 
 
@@ -298,6 +300,8 @@ def run_ours(a, rank, world, local, dist, torch):
     case.nnz = g.nnz()
     nb, npml = g.PathCounts()
     assert g.Autotune()
+    if a.bulk_variant >= 0:
+        assert g.SetBulkVariant(a.bulk_variant)
     tuning = g.Tuning()
     # warm-up
     for _ in range(a.warmup):
