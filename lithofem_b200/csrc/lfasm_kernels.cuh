@@ -188,18 +188,44 @@ k_bulk(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   const double fc0 = c0 ? 1.0 : 0.0, fc1 = c1 ? 1.0 : 0.0;
   const int i0 = blockIdx.x * chunk;
   const int i1 = min(nb, i0 + chunk);
+  // records of the next batch are loaded into registers while the current
+  // batch is computed (BULK_EB * REC <= 2 * BULK_THREADS)
+  constexpr int PF = (BULK_EB * REC + BULK_THREADS - 1) / BULK_THREADS;
+  double pf[PF];
+  int pfe = -1;
+  unsigned pfo = 0u;
+  unsigned long long psm = 0ull, pem = 0ull;
+  auto prefetch = [&](int ib) {
+    const int nbat = min(BULK_EB, i1 - ib);
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int j = tid + u * BULK_THREADS;
+      pf[u] = (ib < i1 && j < nbat * REC) ? rec[(size_t)ib * REC + j] : 0.0;
+    }
+    pfe = (ib < i1 && tid < nbat) ? list[ib + tid] : -1;
+    if (pfe >= 0) {
+      pfo = fopack[pfe];
+      psm = MODE == 1 ? signmask[pfe] : 0ull;
+      pem = (MODE == 1 && eliminate) ? essmask[pfe] : 0ull;
+    }
+  };
+  prefetch(i0);
   for (int ib = i0; ib < i1; ib += BULK_EB) {
     const int nbat = min(BULK_EB, i1 - ib);
     __syncthreads();
-    for (int j = tid; j < nbat * REC; j += BULK_THREADS) sg[j] = rec[(size_t)ib * REC + j];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int j = tid + u * BULK_THREADS;
+      if (j < BULK_EB * REC) sg[j] = pf[u];
+    }
     if (tid < nbat) {
-      const int e = list[ib + tid];
-      se[tid] = e;
-      sfo[tid] = fopack[e];
-      ssm[tid] = MODE == 1 ? signmask[e] : 0ull;
-      sem[tid] = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+      se[tid] = pfe;
+      sfo[tid] = pfo;
+      ssm[tid] = psm;
+      sem[tid] = pem;
     }
     __syncthreads();
+    prefetch(ib + BULK_EB);
     for (int b = 0; b < nbat; ++b) {
       const double *g = sg + b * REC;
       double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
