@@ -416,7 +416,8 @@ def run_ours(a, rank, world, local, dist, torch):
             "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
-            "tuning": {"bulk_variant": ["k_bulk (SIMT)", "k_bulk_mma (DMMA)"][tuning[0]],
+            "tuning": {"bulk_variant": ["k_bulk (SIMT)", "k_bulk_mma<4 tiles/warp> (DMMA)",
+                                        "k_bulk_mma<2 tiles/warp> (DMMA)"][tuning[0]],
                        "bulk_ms": tuning[1]}}
     print(json.dumps(line), flush=True)
     g.Release()

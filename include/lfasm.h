@@ -225,13 +225,14 @@ int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts,
 int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_parts,
                        const void *d_u, const void *d_lambda, void *d_grad);
 
-/* Autotuner: times the bulk-element kernel variants (SIMT k_bulk and the
- * FP64 tensor-core k_bulk_mma) on this mesh and keeps the faster one; runs
- * automatically on the first lfasm_assemble unless a variant was set.
- * lfasm_get_tuning reports the choice and the two timings (ms). */
+/* Autotuner: times the bulk-element kernel variants on this mesh -- 0: the
+ * SIMT k_bulk, 1 and 2: the FP64 tensor-core k_bulk_mma with 4 or 2 tiles
+ * per warp -- and keeps the fastest; runs automatically on the first
+ * lfasm_assemble unless a variant was set.  lfasm_get_tuning reports the
+ * choice and the three timings (ms). */
 int lfasm_autotune(lfasm_handle *h);
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant);
-int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms2);
+int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3);
 
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):

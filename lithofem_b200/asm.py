@@ -98,12 +98,13 @@ class AsmGpu:
         return self._ok(_lib.lib().lfasm_autotune(self._h))
 
     def SetBulkVariant(self, variant: int) -> bool:
-        """0: SIMT bulk-element kernel, 1: FP64 tensor-core (DMMA) variant."""
+        """0: SIMT bulk-element kernel; 1, 2: FP64 tensor-core (DMMA) variant
+        with 4 or 2 tiles per warp."""
         return self._ok(_lib.lib().lfasm_set_bulk_variant(self._h, int(variant)))
 
     def Tuning(self) -> tuple[int, list[float]]:
         v = ct.c_int()
-        ms = (ct.c_float * 2)()
+        ms = (ct.c_float * 3)()
         _lib.check(_lib.lib().lfasm_get_tuning(self._h, ct.byref(v), ms))
         return v.value, [float(x) for x in ms]
 

@@ -103,10 +103,10 @@ struct lfasm_handle {
   double *rec = nullptr;
   // tensor-core bulk variant and the autotuned choice
   double *S_mma = nullptr, *rec_mma = nullptr;
-  int bulk_variant = 0;      // 0: k_bulk (SIMT), 1: k_bulk_mma (DMMA)
+  int bulk_variant = 0;      // 0: k_bulk (SIMT), 1/2: k_bulk_mma (DMMA, 4/2 tiles per warp)
   int tuned = 0;             // autotune done
   int forced = 0;            // variant fixed by lfasm_set_bulk_variant
-  float tune_ms[2] = {0.f, 0.f};
+  float tune_ms[3] = {0.f, 0.f, 0.f};
   dcplx *Ae = nullptr;
   // RHS data
   int *slab_of = nullptr;
@@ -626,19 +626,25 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
                                                              h->rec_mma);
     LF_LAUNCHED();
     const int ntiles = bulk_tiles(h->ndp);
-    const int ytiles = (ntiles + BULK_WARPS * BULK_T - 1) / (BULK_WARPS * BULK_T);
+    const int TT = h->bulk_variant == 1 ? 4 : 2;  // tiles per warp
+    const int ytiles = (ntiles + BULK_WARPS * TT - 1) / (BULK_WARPS * TT);
     // k_bulk_mma writes 16-byte-aligned double4 pairs: needs rs even (the
     // fused layout); the dense ComputeLocal layout uses the SIMT kernel
     const int nbat = (nb + 7) / 8;
     const long long want = (long long)h->sm_count * 8;
     const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
     dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
-#define LF_BULKM(C, M)                                                            \
-  k_bulk_mma<C, M><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                      \
+#define LF_BULKM(C, M, T)                                                         \
+  k_bulk_mma<C, M, T><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                   \
       nb, h->bulk_list, h->rec_mma, h->S_mma, ntiles, h->nd, h->ndp, h->p, bchunk, \
       te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
-    if (cross) { if (mode) LF_BULKM(true, 1); else LF_BULKM(true, 0); }
-    else { if (mode) LF_BULKM(false, 1); else LF_BULKM(false, 0); }
+    if (TT == 4) {
+      if (cross) { if (mode) LF_BULKM(true, 1, 4); else LF_BULKM(true, 0, 4); }
+      else { if (mode) LF_BULKM(false, 1, 4); else LF_BULKM(false, 0, 4); }
+    } else {
+      if (cross) { if (mode) LF_BULKM(true, 1, 2); else LF_BULKM(true, 0, 2); }
+      else { if (mode) LF_BULKM(false, 1, 2); else LF_BULKM(false, 0, 2); }
+    }
 #undef LF_BULKM
     LF_LAUNCHED();
   }
@@ -854,7 +860,7 @@ int lfasm_autotune(lfasm_handle *h) {
   const int keep_n_pml = h->n_pml;
   h->n_pml = 0;  // time the bulk path alone
   int rc = LFASM_OK;
-  for (int v = 0; v < 2 && !rc; ++v) {
+  for (int v = 0; v < 3 && !rc; ++v) {
     h->bulk_variant = v;
     for (int rep = 0; rep < 2 && !rc; ++rep) {
       LF_CUDA(cudaEventRecord(a, h->stream));
@@ -870,7 +876,10 @@ int lfasm_autotune(lfasm_handle *h) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (rc) return rc;
-  h->bulk_variant = h->tune_ms[1] < h->tune_ms[0] ? 1 : 0;
+  int best = 0;
+  for (int v = 1; v < 3; ++v)
+    if (h->tune_ms[v] < h->tune_ms[best]) best = v;
+  h->bulk_variant = best;
   h->tuned = 1;
   h->locals_valid = 0;
   return sync_if(h);
@@ -878,17 +887,17 @@ int lfasm_autotune(lfasm_handle *h) {
 
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
-  if (variant < 0 || variant > 1) return fail(LFASM_ERR_ARG, "bulk variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return fail(LFASM_ERR_ARG, "bulk variant must be 0, 1 or 2");
   h->bulk_variant = variant;
   h->forced = 1;
   h->tuned = 1;
   return LFASM_OK;
 }
 
-int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms2) {
+int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   if (bulk_variant) *bulk_variant = h->bulk_variant;
-  if (ms2) { ms2[0] = h->tune_ms[0]; ms2[1] = h->tune_ms[1]; }
+  if (ms3) for (int i = 0; i < 3; ++i) ms3[i] = h->tune_ms[i];
   return LFASM_OK;
 }
 

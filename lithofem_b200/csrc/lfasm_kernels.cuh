@@ -403,7 +403,7 @@ __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
 // element is one full 128-byte line of the (row-padded) element matrix.  A
 // warp owns BULK_T/2 row-pair blocks (I, cb), i.e. both rows of each pair:
 // the row transform is thread-local, the column pair is thread-local.
-template <bool CROSS, int MODE>
+template <bool CROSS, int MODE, int TT>
 __global__ void __launch_bounds__(BULK_WARPS * 32)
 k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
            const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
@@ -415,7 +415,7 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   __shared__ int se[8];
   __shared__ unsigned sfo[8];
   __shared__ unsigned long long ssm[8], sem[8];
-  constexpr int PB = BULK_T / 2;           // row-pair blocks per warp
+  constexpr int PB = TT / 2;               // row-pair blocks per warp
   constexpr int KS = BK / 4;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
@@ -445,20 +445,44 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   }
   const int nbat = (nb + 7) / 8;
   const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
-  for (int bt = b0; bt < b1; ++bt) {
+  // the next batch's records and element metadata are loaded into registers
+  // while the current batch is computed
+  constexpr int PF = (8 * BREC + BULK_WARPS * 32 - 1) / (BULK_WARPS * 32);
+  double pf[PF];
+  int pfe = -1;
+  unsigned pfo = 0u;
+  unsigned long long psm = 0ull, pem = 0ull;
+  auto prefetch = [&](int bt) {
     const int ebase = bt * 8;
-    const int nel = min(8, nb - ebase);
+    const int nel = bt < b1 ? min(8, nb - ebase) : 0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int j = tid + u * BULK_WARPS * 32;
+      pf[u] = (j < 8 * BREC && (j / BREC) < nel) ? rec[(size_t)ebase * BREC + j] : 0.0;
+    }
+    pfe = tid < nel ? list[ebase + tid] : -1;
+    if (pfe >= 0) {
+      pfo = fopack[pfe];
+      psm = MODE == 1 ? signmask[pfe] : 0ull;
+      pem = (MODE == 1 && eliminate) ? essmask[pfe] : 0ull;
+    }
+  };
+  prefetch(b0);
+  for (int bt = b0; bt < b1; ++bt) {
     __syncthreads();
-    for (int j = tid; j < 8 * BREC; j += BULK_WARPS * 32)
-      sA[j] = (j / BREC) < nel ? rec[(size_t)ebase * BREC + j] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int j = tid + u * BULK_WARPS * 32;
+      if (j < 8 * BREC) sA[j] = pf[u];
+    }
     if (tid < 8) {
-      const int e = tid < nel ? list[ebase + tid] : -1;
-      se[tid] = e;
-      sfo[tid] = e >= 0 ? fopack[e] : 0u;
-      ssm[tid] = (MODE == 1 && e >= 0) ? signmask[e] : 0ull;
-      sem[tid] = (MODE == 1 && e >= 0 && eliminate) ? essmask[e] : 0ull;
+      se[tid] = pfe;
+      sfo[tid] = pfe >= 0 ? pfo : 0u;
+      ssm[tid] = pfe >= 0 ? psm : 0ull;
+      sem[tid] = pfe >= 0 ? pem : 0ull;
     }
     __syncthreads();
+    prefetch(bt + 1);
     double ar[3], ai[KS];
 #pragma unroll
     for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * BREC + ks * 4 + t4];

@@ -225,7 +225,7 @@ def test_against_reference_cuda_kernels(kcase):
 
 
 @pytest.mark.parametrize("kcase", [("grating", 3, 6.0), ("hole", 2, 0.0), ("hole", 1, 6.0), ("slab", 3, 6.0)], ids=ids)
-@pytest.mark.parametrize("variant", [0, 1], ids=["simt", "dmma"])
+@pytest.mark.parametrize("variant", [0, 1, 2], ids=["simt", "dmma4", "dmma2"])
 def test_bulk_variants(kcase, variant):
     """Both bulk-element kernels (the autotuner's candidates) match the oracle."""
     c = case(*kcase) if kcase[0] != "slab" else configs.small_case("slab", 3, 6.0, seed=13, h=3.2)
