@@ -250,4 +250,4 @@ def test_autotuner_picks_a_variant():
     g = AsmGpuGlobal(c.prob)
     assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
     v, ms = g.Tuning()
-    assert v in (0, 1) and ms[0] > 0 and ms[1] > 0 and ms[v] == min(ms)
+    assert v in (0, 1, 2) and min(ms) > 0 and ms[v] == min(ms)
