@@ -14,7 +14,9 @@
  *     one "asm_gpu: CUDA error '<msg>' at <file>:<line>" line, the reference's
  *     diagnostic (asm_gpu.inc:255-263);
  *   - plain pointers and sizes only; host arrays are read during the call;
- *   - device buffers are owned by the handle and freed by lfasm_destroy; the
+ *   - device buffers are owned by the handle and freed by lfasm_destroy
+ *     into a per-device memory pool of the library, which keeps the blocks
+ *     for the next handle (lfasm_trim_pool hands them back to the driver); the
  *     device CSR returned by lfasm_get_csr is borrowed (the cuDSS contract of
  *     solver/cudss_solver.inc:75-110: int32 0-based row pointer, sorted int32
  *     columns, interleaved complex128 {re, im} values, general matrix);
@@ -227,9 +229,12 @@ int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_
 
 /* Autotuner: times the bulk-element kernel variants on this mesh -- 0: the
  * SIMT k_bulk, 1 and 2: the FP64 tensor-core k_bulk_mma with 4 or 2 tiles
- * per warp -- and keeps the fastest; runs automatically on the first
- * lfasm_assemble unless a variant was set.  lfasm_get_tuning reports the
- * choice and the three timings (ms). */
+ * per warp -- and keeps the fastest.  The first lfasm_assemble of a handle
+ * whose variant was not set takes the decision from a per-process cache
+ * keyed by device, order p, k-parallel terms and the power-of-two class of
+ * the bulk element count, and runs the autotuner only on a miss; an explicit
+ * lfasm_autotune always times and refreshes the cache.  lfasm_get_tuning
+ * reports the choice and the three timings (ms). */
 int lfasm_autotune(lfasm_handle *h);
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant);
 int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3);
@@ -247,6 +252,12 @@ int lfasm_stage_times(lfasm_handle *h, float *ms3);
 int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml);
 
 void lfasm_destroy(lfasm_handle *h);
+
+/* Hands the device memory cached by the library's pool on device gpu_id
+ * (blocks of destroyed handles and temporaries) back to the driver; live
+ * handles keep theirs.  No counterpart in the reference, whose handles
+ * cudaMalloc and cudaFree their buffers directly. */
+int lfasm_trim_pool(int gpu_id);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,7 @@ def lib() -> ct.CDLL:
         "lfasm_set_bulk_variant": (ct.c_int, [H, ct.c_int]),
         "lfasm_get_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
+        "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

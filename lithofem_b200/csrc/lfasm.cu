@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <atomic>
 #include <mutex>
 #include <cmath>
@@ -57,18 +59,67 @@ int fail(int code, const char *fmt, ...) {
 
 #define LF_LAUNCHED() g_launches.fetch_add(1, std::memory_order_relaxed)
 
+// Device memory of the handles comes from one stream-ordered pool per
+// device, owned by the library, whose release threshold keeps freed blocks:
+// the multi-GB element and value buffers of a destroyed handle are handed to
+// the next handle without a cudaMalloc/cudaFree round trip to the driver.
+// Allocations and frees are ordered on the legacy default stream;
+// lfasm_trim_pool returns the cached blocks to the driver.
+constexpr int MAX_DEV = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[MAX_DEV] = {};
+
+cudaError_t dev_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if ((e = cudaMemPoolCreate(&pool, &pp)) != cudaSuccess) return e;
+    unsigned long long keep = ~0ull;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t dmalloc(T *&dst, size_t count) {
+  dst = nullptr;
+  cudaMemPool_t pool;
+  cudaError_t e = dev_pool(&pool);
+  if (e != cudaSuccess) return e;
+  void *p = nullptr;
+  if ((e = cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, 0)) != cudaSuccess)
+    return e;
+  dst = static_cast<T *>(p);
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t upload(T *&dst, const T *src, size_t count) {
   dst = nullptr;
   if (count == 0) return cudaSuccess;
-  cudaError_t e = cudaMalloc(&dst, count * sizeof(T));
+  cudaError_t e = dmalloc(dst, count);
   if (e != cudaSuccess) return e;
   return cudaMemcpy(dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
 }
 
 template <typename T>
 void dfree(T *&p) {
-  if (p) { cudaFree((void *)p); p = nullptr; }
+  if (p) { cudaFreeAsync((void *)p, 0); p = nullptr; }
 }
 
 struct DevRule {
@@ -320,6 +371,9 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
       !ad->rule_cc.curl || !ad->rule_mass.curl || !ad->rule_mass.vshape || !ad->rule_cc.w ||
       !ad->rule_mass.w)
     return fail(LFASM_ERR_ARG, "missing reference rule tables");
+  if (ad->rule_cc.nq + ad->rule_mass.nq > PML_MAXQ)
+    return fail(LFASM_ERR_UNSUPPORTED, "%d + %d quadrature points exceed the %d per element supported",
+                ad->rule_cc.nq, ad->rule_mass.nq, PML_MAXQ);
   if (prob->n_regions <= 0 || !prob->region_eps || !prob->region_kind)
     return fail(LFASM_ERR_ARG, "missing region table");
   if (!(prob->pml_thick > 0.0) || !(prob->k0 > 0.0))
@@ -466,7 +520,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   h->n_pml = (int)pl.size();
   LF_CUDA_H(upload(h->bulk_list, bl.data(), bl.size()));
   LF_CUDA_H(upload(h->pml_list, pl.data(), pl.size()));
-  if (h->n_bulk) LF_CUDA_H(cudaMalloc(&h->rec, (size_t)h->n_bulk * REC * sizeof(double)));
+  if (h->n_bulk) LF_CUDA_H(dmalloc(h->rec, (size_t)h->n_bulk * REC));
 
   std::vector<double> S;
   build_S(ad, h->ndp, S);
@@ -474,7 +528,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   build_S_mma(ad, h->ndp, S);
   LF_CUDA_H(upload(h->S_mma, S.data(), S.size()));
   if (h->n_bulk)
-    LF_CUDA_H(cudaMalloc(&h->rec_mma, (size_t)h->n_bulk * BREC * sizeof(double)));
+    LF_CUDA_H(dmalloc(h->rec_mma, (size_t)h->n_bulk * BREC));
 
   // RHS source elements: frustum regions (delta = region eps - eps_bg) or,
   // with per-element eps, every non-PML element whose eps differs from its
@@ -522,7 +576,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   // element buffer: dense nd x nd rows for lfasm_compute_local, padded row
   // stride ndp (even) for the fused path so every row starts on a 32-byte
   // sector and column pairs fill whole sectors
-  LF_CUDA_H(cudaMalloc(&h->Ae, ne * nd * h->rs * sizeof(dcplx)));
+  LF_CUDA_H(dmalloc(h->Ae, ne * nd * h->rs));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
   LF_CUDA_H(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   LF_CUDA_H(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
@@ -701,24 +755,25 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
   const int n = h->n, nd = h->nd;
   const long long total = (long long)h->ne * nd;
   int *cnt = nullptr, *fill = nullptr, *dmax = nullptr, *err = nullptr;
-  void *tmp = nullptr;
+  int *tmpJ = nullptr;  // every row's unique columns at its candidate offset
+  unsigned char *tmp = nullptr;
   size_t tmp_bytes = 0;
-  LF_CUDA(cudaMalloc(&cnt, (size_t)(n + 1) * sizeof(int)));
-  LF_CUDA(cudaMalloc(&fill, (size_t)n * sizeof(int)));
-  LF_CUDA(cudaMalloc(&dmax, 2 * sizeof(int)));
-  LF_CUDA(cudaMalloc(&err, sizeof(int)));
+  LF_CUDA(dmalloc(cnt, (size_t)(n + 1)));
+  LF_CUDA(dmalloc(fill, (size_t)n));
+  LF_CUDA(dmalloc(dmax, 2));
+  LF_CUDA(dmalloc(err, 1));
   LF_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(n + 1) * sizeof(int), h->stream));
   LF_CUDA(cudaMemsetAsync(fill, 0, (size_t)n * sizeof(int), h->stream));
   LF_CUDA(cudaMemsetAsync(dmax, 0, 2 * sizeof(int), h->stream));
   LF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), h->stream));
-  LF_CUDA(cudaMalloc(&h->ea_ptr, (size_t)(n + 1) * sizeof(int)));
-  LF_CUDA(cudaMalloc(&h->ea, (size_t)total * sizeof(int)));
+  LF_CUDA(dmalloc(h->ea_ptr, (size_t)(n + 1)));
+  LF_CUDA(dmalloc(h->ea, (size_t)total));
   const int tb = 256;
   const unsigned gb = (unsigned)((total + tb - 1) / tb);
   k_count_rows<<<gb, tb, 0, h->stream>>>(total, h->dof, cnt);
   LF_LAUNCHED();
   LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, h->ea_ptr, n + 1, h->stream));
-  LF_CUDA(cudaMalloc(&tmp, tmp_bytes));
+  LF_CUDA(dmalloc(tmp, tmp_bytes));
   LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, h->ea_ptr, n + 1, h->stream));
   k_fill_rows<<<gb, tb, 0, h->stream>>>(total, h->dof, h->ea_ptr, fill, h->ea);
   LF_LAUNCHED();
@@ -728,7 +783,7 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
   LF_CUDA(cudaMemcpyAsync(&mmax, dmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   LF_CUDA(cudaStreamSynchronize(h->stream));
   if (mmax > 64) {
-    cudaFree(cnt); cudaFree(fill); cudaFree(dmax); cudaFree(err); cudaFree(tmp);
+    dfree(cnt); dfree(fill); dfree(dmax); dfree(err); dfree(tmp);
     return fail(LFASM_ERR_UNSUPPORTED, "a dof belongs to %d elements (max 64)", mmax);
   }
   int cap = 32;
@@ -736,38 +791,32 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
   const int wpb = 4;
   const size_t smem = (size_t)wpb * (cap + 64) * sizeof(int);
   const unsigned rb = (unsigned)((n + wpb - 1) / wpb);
-  LF_CUDA(cudaMalloc(&h->off, (size_t)total * nd * sizeof(uint16_t)));
+  LF_CUDA(dmalloc(h->off, (size_t)total * nd));
   if (!hI) {
+    LF_CUDA(dmalloc(tmpJ, (size_t)total * nd));
     LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_row_symbolic<1><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
-                                                          cnt, nullptr, nullptr, nullptr, err);
+                                                          cnt, nullptr, nullptr, tmpJ, h->off, err);
     LF_LAUNCHED();
-    LF_CUDA(cudaMalloc(&h->I, (size_t)(n + 1) * sizeof(int)));
+    LF_CUDA(dmalloc(h->I, (size_t)(n + 1)));
     LF_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int), h->stream));
     LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, h->I, n + 1, h->stream));
     int nnz = 0;
     LF_CUDA(cudaMemcpyAsync(&nnz, h->I + n, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     LF_CUDA(cudaStreamSynchronize(h->stream));
     h->nnz = nnz;
-    LF_CUDA(cudaMalloc(&h->Jc, (size_t)std::max(nnz, 1) * sizeof(int)));
-    k_row_symbolic<2><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
-                                                          nullptr, h->I, h->Jc, h->off, err);
+    LF_CUDA(dmalloc(h->Jc, (size_t)std::max(nnz, 1)));
+    k_row_compact<<<(unsigned)((n + 7) / 8), 256, 0, h->stream>>>(n, nd, h->ea_ptr, h->I, tmpJ,
+                                                                   h->Jc);
     LF_LAUNCHED();
   } else {
-    // sort each row's list (pass 1 without counting) then map into the
-    // caller's sparsity
-    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_row_symbolic<1><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
-                                                          cnt, nullptr, nullptr, nullptr, err);
-    LF_LAUNCHED();
+    // map every row's candidates into the caller's sparsity
     h->nnz = nnz_given;
     LF_CUDA(upload(h->I, hI, (size_t)n + 1));
     LF_CUDA(upload(h->Jc, hJ, (size_t)nnz_given));
-    const size_t smem3 = (size_t)wpb * (cap + 64) * sizeof(int);
-    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
-    k_row_symbolic<3><<<rb, wpb * 32, smem3, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
-                                                           nullptr, h->I, h->Jc, h->off, err);
+    LF_CUDA(cudaFuncSetAttribute(k_row_symbolic<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_row_symbolic<3><<<rb, wpb * 32, smem, h->stream>>>(n, nd, h->dof, h->ea_ptr, h->ea, cap,
+                                                          nullptr, h->I, h->Jc, nullptr, h->off, err);
     LF_LAUNCHED();
   }
   k_max_reduce<<<256, 256, 0, h->stream>>>(n, h->I, 1, dmax + 1);
@@ -776,7 +825,7 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
   LF_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   LF_CUDA(cudaMemcpyAsync(&mrow, dmax + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   LF_CUDA(cudaStreamSynchronize(h->stream));
-  cudaFree(cnt); cudaFree(fill); cudaFree(dmax); cudaFree(err); cudaFree(tmp);
+  dfree(cnt); dfree(fill); dfree(dmax); dfree(err); dfree(tmp); dfree(tmpJ);
   if (herr == 1) return fail(LFASM_ERR_CSR, "CSR position missing: the given sparsity lacks an element coupling");
   if (herr) return fail(LFASM_ERR_UNSUPPORTED, "row map overflow");
   if (mrow > 65535) return fail(LFASM_ERR_UNSUPPORTED, "row with %d entries exceeds 65535", mrow);
@@ -787,10 +836,10 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
 static int build_global_csr(lfasm_handle *h, const int *hI, const int *hJ, long long nnz) {
   int rc = build_maps(h, hI, hJ, nnz);
   if (rc) return rc;
-  LF_CUDA(cudaMalloc(&h->vals, (size_t)std::max<long long>(h->nnz, 1) * sizeof(dcplx)));
+  LF_CUDA(dmalloc(h->vals, (size_t)std::max<long long>(h->nnz, 1)));
   h->n_part_blocks = (h->n + 7) / 8;
-  LF_CUDA(cudaMalloc(&h->partials, (size_t)h->n_part_blocks * 2 * sizeof(double)));
-  LF_CUDA(cudaMalloc(&h->red, 2 * sizeof(double)));
+  LF_CUDA(dmalloc(h->partials, (size_t)h->n_part_blocks * 2));
+  LF_CUDA(dmalloc(h->red, 2));
   h->built = 1;
   return sync_if(h);
 }
@@ -810,7 +859,7 @@ int lfasm_build_global(lfasm_handle *h, const int *ess_list, int n_ess) {
     ess[ess_list[i]] = 1;
   }
   LF_CUDA(upload(h->ess, ess.data(), ess.size()));
-  LF_CUDA(cudaMalloc(&h->essmask, (size_t)h->ne * sizeof(unsigned long long)));
+  LF_CUDA(dmalloc(h->essmask, (size_t)h->ne));
   k_essmask<<<(h->ne + 255) / 256, 256, 0, h->stream>>>(h->ne, h->nd, h->dof, h->ess, h->essmask);
   LF_LAUNCHED();
   if (h->h_I.empty()) return build_global_csr(h, nullptr, nullptr, 0);
@@ -847,6 +896,27 @@ int lfasm_scatter_eliminate(lfasm_handle *h, int eliminate) {
   return sync_if(h);
 }
 
+}  // extern "C"
+
+// Per-process cache of autotuner decisions, keyed by device, order p,
+// k-parallel terms and the power-of-two class of the bulk element count.
+namespace {
+struct TuneEntry {
+  int variant;
+  float ms[3];
+};
+std::mutex g_tune_mu;
+std::map<std::array<int, 4>, TuneEntry> g_tune;
+
+std::array<int, 4> tune_key(const lfasm_handle *h) {
+  int cls = 0;
+  while ((1 << cls) < h->n_bulk && cls < 30) ++cls;
+  return {h->dev, h->p, h->has_kpar, cls};
+}
+}  // namespace
+
+extern "C" {
+
 // Autotuner: times each bulk-element variant on this mesh (two launches
 // each, the second timed with CUDA events) and keeps the faster one.
 int lfasm_autotune(lfasm_handle *h) {
@@ -882,6 +952,12 @@ int lfasm_autotune(lfasm_handle *h) {
   h->bulk_variant = best;
   h->tuned = 1;
   h->locals_valid = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    TuneEntry &t = g_tune[tune_key(h)];
+    t.variant = best;
+    for (int v = 0; v < 3; ++v) t.ms[v] = h->tune_ms[v];
+  }
   return sync_if(h);
 }
 
@@ -906,8 +982,21 @@ int lfasm_assemble(lfasm_handle *h, int eliminate) {
   g_err.clear();
   if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
   if (!h->tuned) {
-    int rt = lfasm_autotune(h);
-    if (rt) return rt;
+    bool hit = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(tune_key(h));
+      if (it != g_tune.end()) {
+        hit = true;
+        h->bulk_variant = it->second.variant;
+        for (int v = 0; v < 3; ++v) h->tune_ms[v] = it->second.ms[v];
+        h->tuned = 1;
+      }
+    }
+    if (!hit) {
+      int rt = lfasm_autotune(h);
+      if (rt) return rt;
+    }
   }
   const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
   int rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, eliminate ? 1 : 0);
@@ -992,9 +1081,9 @@ int lfasm_residual(lfasm_handle *h, const double *X, const double *B, double *re
   double *d2 = nullptr;
   dcplx *dx = nullptr, *db = nullptr;
   const size_t n = h->n;
-  LF_CUDA(cudaMalloc(&d2, 2 * n * sizeof(double)));
-  LF_CUDA(cudaMalloc(&dx, n * sizeof(dcplx)));
-  LF_CUDA(cudaMalloc(&db, n * sizeof(dcplx)));
+  LF_CUDA(dmalloc(d2, 2 * n));
+  LF_CUDA(dmalloc(dx, n));
+  LF_CUDA(dmalloc(db, n));
   const unsigned g = (unsigned)((n + 255) / 256);
   LF_CUDA(cudaMemcpyAsync(d2, X, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   k_split_to_cplx<<<g, 256, 0, h->stream>>>((int)n, d2, dx);
@@ -1003,9 +1092,9 @@ int lfasm_residual(lfasm_handle *h, const double *X, const double *B, double *re
   k_split_to_cplx<<<g, 256, 0, h->stream>>>((int)n, d2, db);
   LF_LAUNCHED();
   int rc = residual_core(h, dx, db, rel);
-  cudaFree(d2);
-  cudaFree(dx);
-  cudaFree(db);
+  dfree(d2);
+  dfree(dx);
+  dfree(db);
   return rc;
 }
 
@@ -1135,7 +1224,7 @@ int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts, int n_
   LF_CUDA(upload(dw, waves.data(), waves.size()));
   std::vector<int> cols(col_of_part, col_of_part + n_parts);
   if (n_parts) LF_CUDA(upload(dcol, cols.data(), cols.size()));
-  if (h->n_src) LF_CUDA(cudaMalloc(&be, (size_t)h->n_src * ncol * h->nd * sizeof(dcplx)));
+  if (h->n_src) LF_CUDA(dmalloc(be, (size_t)h->n_src * ncol * h->nd));
   if (h->n_src && n_parts) {
     const int wpb = 4;
     k_rhs_elem<<<(h->n_src + wpb - 1) / wpb, wpb * 32, 0, h->stream>>>(
@@ -1150,9 +1239,9 @@ int lfasm_assemble_rhs(lfasm_handle *h, const lfasm_incident_part *parts, int n_
                                                           eliminate ? 1 : 0, (dcplx *)d_b);
   LF_LAUNCHED();
   LF_CUDA(cudaStreamSynchronize(h->stream));
-  cudaFree(dw);
-  if (dcol) cudaFree(dcol);
-  if (be) cudaFree(be);
+  dfree(dw);
+  dfree(dcol);
+  dfree(be);
   return sync_if(h);
 }
 
@@ -1205,13 +1294,17 @@ int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_
     LF_LAUNCHED();
   }
   LF_CUDA(cudaStreamSynchronize(h->stream));
-  cudaFree(dw);
+  dfree(dw);
   return sync_if(h);
 }
 
 void lfasm_destroy(lfasm_handle *h) {
   if (!h) return;
   cudaSetDevice(h->dev);
+  // the buffers go back to the pool on the legacy stream: the handle's own
+  // streams (possibly non-blocking) finish first
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->side) cudaStreamSynchronize(h->side);
   dfree(h->dof); dfree(h->sign); dfree(h->attr); dfree(h->J); dfree(h->Jinv); dfree(h->detJ);
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
   for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
@@ -1226,6 +1319,24 @@ void lfasm_destroy(lfasm_handle *h) {
   if (h->join) cudaEventDestroy(h->join);
   if (h->side) cudaStreamDestroy(h->side);
   delete h;
+}
+
+int lfasm_trim_pool(int gpu_id) {
+  if (gpu_id < 0 || gpu_id >= MAX_DEV) return fail(LFASM_ERR_ARG, "gpu_id %d out of range", gpu_id);
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    pool = g_pool[gpu_id];
+  }
+  if (!pool) return LFASM_OK;
+  int cur = 0;
+  LF_CUDA(cudaGetDevice(&cur));
+  LF_CUDA(cudaSetDevice(gpu_id));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  cudaSetDevice(cur);
+  LF_CUDA(e);
+  return LFASM_OK;
 }
 
 }  // extern "C"

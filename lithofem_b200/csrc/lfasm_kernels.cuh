@@ -561,8 +561,14 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 // to 8).  One warp per 8-column tile (real and imaginary planes), all
 // M tiles, so the epilogue holds both parts of each entry.  Rows are staged
 // in chunks of PML_QC points; blocks are persistent over the PML elements.
+//
+// The stretch coefficients of every point of both rules (one pow() each)
+// are formed once per element by all threads in parallel, into a table in
+// shared memory; each chunk then needs two block barriers (rows staged /
+// rows consumed).
 // ---------------------------------------------------------------------------
-constexpr int PML_QC = 8;  // quadrature points staged per round
+constexpr int PML_QC = 8;     // quadrature points staged per round
+constexpr int PML_MAXQ = 40;  // cc-rule + mass-rule points per element (p = 3: 11 + 24)
 
 struct QCoef {  // per quadrature point, already multiplied by w_q detJ
   dcplx a00, a01, a10, a11, a22;      // (Md + M2) entries (cc rule: Lambda^-1 diagonal)
@@ -576,11 +582,57 @@ struct PmlShape {
   static constexpr int MT = NDP8 / 8;                    // row tiles
   static constexpr int LD = (NDP8 % 16 == 0) ? NDP8 + 8 : NDP8;  // row stride = 8 mod 16
   static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
-  static constexpr size_t SMEM = (size_t)3 * RMAX * LD * sizeof(double) + PML_QC * sizeof(QCoef);
+  static constexpr size_t SMEM =
+      (size_t)3 * RMAX * LD * sizeof(double) + PML_MAXQ * sizeof(QCoef);
+  // blocks per SM the register budget is cut for (shared memory allows it)
+  // p = 3 stays at 2 blocks (a 3-block register cap spills and runs slower)
+  static constexpr int MINB = NDP8 >= 48 ? 2 : NDP8 >= 24 ? 4 : 8;
 };
 
+// Coefficients of one quadrature point (rule 0: curl-curl, rule 1: mass and
+// k-parallel terms), asm_gpu.inc:86-161 restated per point.
+__device__ __forceinline__ QCoef pml_qcoef(const PmlParams &pml, int rule, int mask, double z,
+                                          double wq, dcplx eps) {
+  const double k2 = pml.k0 * pml.k0;
+  const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
+  const dcplx s = pml_s(pml, z);
+  const dcplx si = cinv(s);
+  QCoef c;
+  if (rule == 0) {
+    c.a00 = cscale(wq, si); c.a11 = c.a00; c.a22 = cscale(wq, s);
+    c.a01 = mk(0, 0); c.a10 = mk(0, 0);
+    c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
+    return c;
+  }
+  const dcplx li0 = si, li1 = si, li2 = s;
+  dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
+  if (mask & 2) {
+    const dcplx me = cscale(-k2, eps);
+    a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
+  }
+  if (mask & 16) {
+    a00 = cadd(a00, cscale(-K02 * K20, li2));
+    a01 = cadd(a01, cscale(-K02 * K21, li2));
+    a10 = cadd(a10, cscale(-K12 * K20, li2));
+    a11 = cadd(a11, cscale(-K12 * K21, li2));
+    a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
+  }
+  c.a00 = cscale(wq, a00); c.a01 = cscale(wq, a01); c.a10 = cscale(wq, a10);
+  c.a11 = cscale(wq, a11); c.a22 = cscale(wq, a22);
+  const dcplx iu = mk(0.0, 1.0);
+  if (mask & 4) {
+    c.b02 = cscale(wq * K02, cmul(iu, li2)); c.b12 = cscale(wq * K12, cmul(iu, li2));
+    c.b20 = cscale(wq * K20, cmul(iu, li0)); c.b21 = cscale(wq * K21, cmul(iu, li1));
+  } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
+  if (mask & 8) {
+    c.c02 = cscale(wq * K02, cmul(iu, li0)); c.c12 = cscale(wq * K12, cmul(iu, li1));
+    c.c20 = cscale(wq * K20, cmul(iu, li2)); c.c21 = cscale(wq * K21, cmul(iu, li2));
+  } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
+  return c;
+}
+
 template <int NDP8, bool CROSS, int MODE>
-__global__ void __launch_bounds__(NDP8 * 4)
+__global__ void __launch_bounds__(NDP8 * 4, PmlShape<NDP8>::MINB)
 k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
           const double *__restrict__ J9, const double *__restrict__ Ji9,
           const double *__restrict__ detJ, const double *__restrict__ v0,
@@ -595,26 +647,30 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
   double *Xs = smem;
   double *Yr = Xs + RMAX * LD;
   double *Yi = Yr + RMAX * LD;
-  QCoef *qc = reinterpret_cast<QCoef *>(Yi + RMAX * LD);
-  __shared__ double sJ[9], sJi[9], sdet, sv0z;
-  __shared__ dcplx seps;
+  QCoef *qtab = reinterpret_cast<QCoef *>(Yi + RMAX * LD);
+  __shared__ double sJ[9], sJi[9], sidet;
   __shared__ unsigned sfo;
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
-  const double k2 = pml.k0 * pml.k0;
-  const double K02 = pml.ky, K12 = -pml.kx, K20 = -pml.ky, K21 = pml.kx;
   constexpr int npair = NDP8 / 2;
+  const int nq_all = rcc.nq + rm.nq;  // <= PML_MAXQ, checked by the host
 
   for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
     const int e = list[ie];
-    __syncthreads();  // previous element done with the shared scalars
+    // element scalars and the coefficient table; the previous element's
+    // last barrier already ordered every read of both before these writes
     if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
-    if (tid == 0) {
-      sdet = detJ[e];
-      sv0z = v0[(size_t)e * 3 + 2];
-      seps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
-      sfo = fopack[e];
+    if (tid == 0) { sidet = 1.0 / detJ[e]; sfo = fopack[e]; }
+    for (int j = tid; j < nq_all; j += blockDim.x) {
+      const int rule = j < rcc.nq ? 0 : 1;
+      const int q = rule == 0 ? j : j - rcc.nq;
+      const Rule &R = rule == 0 ? rcc : rm;
+      const double *Jz = J9 + (size_t)e * 9 + 6;
+      const double z = v0[(size_t)e * 3 + 2] + Jz[0] * R.ip[q * 3 + 0] +
+                       Jz[1] * R.ip[q * 3 + 1] + Jz[2] * R.ip[q * 3 + 2];
+      const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+      qtab[j] = pml_qcoef(pml, rule, rule == 0 ? mask_cc : mask_mass, z, R.w[q] * detJ[e], eps);
     }
     double cr[MT][2], ci[MT][2];
 #pragma unroll
@@ -625,58 +681,18 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
       const int mask = rule == 0 ? mask_cc : mask_mass;
       if (!mask) continue;
       const Rule R = rule == 0 ? rcc : rm;
+      const QCoef *qc = qtab + (rule == 0 ? 0 : rcc.nq);
       const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
       const bool need_v = rule == 1;
       const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
       for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
         const int nqc = min(PML_QC, R.nq - q0);
         const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
-        if (tid < nqc) {
-          const int q = q0 + tid;
-          const double z = sv0z + sJ[6] * R.ip[q * 3 + 0] + sJ[7] * R.ip[q * 3 + 1] +
-                           sJ[8] * R.ip[q * 3 + 2];
-          const dcplx s = pml_s(pml, z);
-          const dcplx si = cinv(s);
-          const double wq = R.w[q] * sdet;
-          QCoef c;
-          if (rule == 0) {
-            c.a00 = cscale(wq, si); c.a11 = cscale(wq, si); c.a22 = cscale(wq, s);
-            c.a01 = mk(0, 0); c.a10 = mk(0, 0);
-            c.b02 = c.b12 = c.b20 = c.b21 = c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0);
-          } else {
-            const dcplx li0 = si, li1 = si, li2 = s;
-            dcplx a00 = mk(0, 0), a01 = mk(0, 0), a10 = mk(0, 0), a11 = mk(0, 0), a22 = mk(0, 0);
-            if (mask & 2) {
-              const dcplx me = cscale(-k2, seps);
-              a00 = cmul(me, s); a11 = a00; a22 = cmul(me, si);
-            }
-            if (mask & 16) {
-              a00 = cadd(a00, cscale(-K02 * K20, li2));
-              a01 = cadd(a01, cscale(-K02 * K21, li2));
-              a10 = cadd(a10, cscale(-K12 * K20, li2));
-              a11 = cadd(a11, cscale(-K12 * K21, li2));
-              a22 = cadd(a22, cadd(cscale(-K20 * K02, li0), cscale(-K21 * K12, li1)));
-            }
-            c.a00 = cscale(wq, a00); c.a01 = cscale(wq, a01); c.a10 = cscale(wq, a10);
-            c.a11 = cscale(wq, a11); c.a22 = cscale(wq, a22);
-            const dcplx iu = mk(0.0, 1.0);
-            if (mask & 4) {
-              c.b02 = cscale(wq * K02, cmul(iu, li2)); c.b12 = cscale(wq * K12, cmul(iu, li2));
-              c.b20 = cscale(wq * K20, cmul(iu, li0)); c.b21 = cscale(wq * K21, cmul(iu, li1));
-            } else { c.b02 = c.b12 = c.b20 = c.b21 = mk(0, 0); }
-            if (mask & 8) {
-              c.c02 = cscale(wq * K02, cmul(iu, li0)); c.c12 = cscale(wq * K12, cmul(iu, li1));
-              c.c20 = cscale(wq * K20, cmul(iu, li2)); c.c21 = cscale(wq * K21, cmul(iu, li2));
-            } else { c.c02 = c.c12 = c.c20 = c.c21 = mk(0, 0); }
-          }
-          qc[tid] = c;
-        }
         // zero the padding rows up to a multiple of 4
         for (int i = tid; i < (nrows4 - nrows) * LD; i += blockDim.x) {
           const int r = nrows + i / LD, k = i % LD;
           Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
         }
-        __syncthreads();
         for (int it = tid; it < nqc * npair; it += blockDim.x) {
           const int qi = it / npair, pr = it - qi * npair;
           const int q = q0 + qi;
@@ -694,7 +710,7 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
                 if (need_v)
                   v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
                 if (need_c)
-                  c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) / sdet;
+                  c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) * sidet;
               }
             }
           }
@@ -712,7 +728,7 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
               }
             }
           }
-          const QCoef &C = qc[qi];
+          const QCoef &C = qc[q];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int k = 2 * pr + h;
@@ -879,15 +895,20 @@ __global__ void k_max_reduce(int n, const int *__restrict__ ptr, int diff, int *
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-// one warp per row.  PASS 1: sort the row's (element, row) list, count unique
-// columns.  PASS 2: write sorted unique columns and the slot offsets.
+// one warp per row.  Both passes first sort the row's (element, row) list
+// (the gather sums in that order).
+// PASS 1: sort the candidate columns (every dof of every listed element),
+// padded only to the next power of two of this row's own count; write the
+// unique columns to the row's candidate segment of tmpJ (offset
+// ea_ptr[r] * nd, which has room for all candidates), their count and the
+// slot offsets (positions within the row, independent of where it starts).
 // PASS 3: given columns (I/Jcol from the caller): offsets by binary search.
 template <int PASS>
 __global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
                                const int *__restrict__ ea_ptr, int *__restrict__ ea,
                                int cap, int *__restrict__ cnt, const int *__restrict__ I,
-                               int *__restrict__ Jc, uint16_t *__restrict__ off,
-                               int *__restrict__ err) {
+                               const int *__restrict__ Jc, int *__restrict__ tmpJ,
+                               uint16_t *__restrict__ off, int *__restrict__ err) {
   extern __shared__ int sh[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int r = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -896,26 +917,20 @@ __global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
   int *lst = buf + cap;  // up to 64 (element,row) ids
   const int p0 = ea_ptr[r], m = ea_ptr[r + 1] - p0;
   if (m > 64) { if (lane == 0) atomicExch(err, 2); return; }
-  if (PASS == 1) {
-    if (lane < m) lst[lane] = ea[p0 + lane];
-    if (lane + 32 < m) lst[lane + 32] = ea[p0 + lane + 32];
-    __syncwarp();
-    if (lane == 0) {  // insertion sort (m is small)
-      for (int a = 1; a < m; ++a) {
-        const int v = lst[a];
-        int b = a - 1;
-        while (b >= 0 && lst[b] > v) { lst[b + 1] = lst[b]; --b; }
-        lst[b + 1] = v;
-      }
+  if (lane < m) lst[lane] = ea[p0 + lane];
+  if (lane + 32 < m) lst[lane + 32] = ea[p0 + lane + 32];
+  __syncwarp();
+  if (lane == 0) {  // insertion sort (m is small)
+    for (int a = 1; a < m; ++a) {
+      const int v = lst[a];
+      int b = a - 1;
+      while (b >= 0 && lst[b] > v) { lst[b + 1] = lst[b]; --b; }
+      lst[b + 1] = v;
     }
-    __syncwarp();
-    if (lane < m) ea[p0 + lane] = lst[lane];
-    if (lane + 32 < m) ea[p0 + lane + 32] = lst[lane + 32];
-  } else {
-    if (lane < m) lst[lane] = ea[p0 + lane];
-    if (lane + 32 < m) lst[lane + 32] = ea[p0 + lane + 32];
   }
   __syncwarp();
+  if (lane < m) ea[p0 + lane] = lst[lane];
+  if (lane + 32 < m) ea[p0 + lane + 32] = lst[lane + 32];
   const int tot = m * nd;
   if (PASS == 3) {
     const int rb = I[r], re = I[r + 1];
@@ -932,7 +947,9 @@ __global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
     }
     return;
   }
-  for (int i = lane; i < cap; i += 32) {
+  int len = 32;  // this row's sort length; tot <= cap
+  while (len < tot) len <<= 1;
+  for (int i = lane; i < len; i += 32) {
     int v = 0x7fffffff;
     if (i < tot) {
       const int id = lst[i / nd];
@@ -941,48 +958,59 @@ __global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
     buf[i] = v;
   }
   __syncwarp();
-  // bitonic sort (ascending)
-  for (int k = 2; k <= cap; k <<= 1) {
+  // bitonic sort (ascending); each lane takes compare pairs (i, i | j)
+  for (int k = 2; k <= len; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < cap; i += 32) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const int a = buf[i], b = buf[ixj];
-          const bool up = (i & k) == 0;
-          if ((a > b) == up) { buf[i] = b; buf[ixj] = a; }
-        }
+      for (int pi = lane; pi < (len >> 1); pi += 32) {
+        const int i = ((pi & ~(j - 1)) << 1) | (pi & (j - 1));
+        const int ixj = i | j;
+        const int a = buf[i], b = buf[ixj];
+        if ((a > b) == ((i & k) == 0)) { buf[i] = b; buf[ixj] = a; }
       }
       __syncwarp();
     }
   }
-  // unique: count / compact (chunks of 32 with ballot prefix)
-  int base = 0;
-  const int rbase = PASS == 2 ? I[r] : 0;
-  for (int c0 = 0; c0 < cap; c0 += 32) {
-    const int i = c0 + lane;
-    const int v = buf[i];
-    const bool keep = v != 0x7fffffff && (i == 0 || buf[i - 1] != v);
+  // unique, compacted in place (a chunk writes only at or below what it read)
+  int nr = 0, last = -1;
+  for (int c0 = 0; c0 < len; c0 += 32) {
+    const int v = buf[c0 + lane];
+    int prev = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) prev = last;
+    last = __shfl_sync(0xffffffffu, v, 31);
+    const bool keep = v != 0x7fffffff && v != prev;
     const unsigned bal = __ballot_sync(0xffffffffu, keep);
-    if (PASS == 2 && keep) Jc[rbase + base + __popc(bal & ((1u << lane) - 1u))] = v;
-    base += __popc(bal);
+    __syncwarp();
+    if (keep) buf[nr + __popc(bal & ((1u << lane) - 1u))] = v;
+    nr += __popc(bal);
+    __syncwarp();
   }
-  if (PASS == 1) {
-    if (lane == 0) cnt[r] = base;
-    return;
-  }
-  __syncwarp();
-  // offsets: binary search of each candidate in the unique list (global)
-  const int nr = base;
+  if (lane == 0) cnt[r] = nr;
+  int *dst = tmpJ + (size_t)p0 * nd;
+  for (int j = lane; j < nr; j += 32) dst[j] = buf[j];
+  // offsets: binary search of each candidate in the unique list
   for (int i = lane; i < tot; i += 32) {
     const int id = lst[i / nd];
     const int col = dof[(size_t)(id / nd) * nd + (i % nd)];
     int lo = 0, hi = nr - 1;
     while (lo < hi) {
       const int mid = (lo + hi) >> 1;
-      if (Jc[rbase + mid] < col) lo = mid + 1; else hi = mid;
+      if (buf[mid] < col) lo = mid + 1; else hi = mid;
     }
     off[(size_t)p0 * nd + i] = (uint16_t)lo;
   }
+}
+
+// one warp per row: the row's unique columns from its candidate segment of
+// tmpJ into the final CSR column array
+__global__ void k_row_compact(int n, int nd, const int *__restrict__ ea_ptr,
+                              const int *__restrict__ I, const int *__restrict__ tmpJ,
+                              int *__restrict__ Jc) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= n) return;
+  const int *src = tmpJ + (size_t)ea_ptr[r] * nd;
+  const int rb = I[r], len = I[r + 1] - rb;
+  for (int j = lane; j < len; j += 32) Jc[rb + j] = src[j];
 }
 
 __global__ void k_essmask(int ne, int nd, const int *__restrict__ dof,

@@ -15,7 +15,7 @@ import copy
 import numpy as np
 import pytest
 
-from lithofem_b200 import configs
+from lithofem_b200 import _lib, configs
 from lithofem_b200.asm import CROSS0, CROSS1, CURLCURL, KLK, MASS, AsmGpu, AsmGpuGlobal
 from oracle import oracle
 
@@ -251,3 +251,20 @@ def test_autotuner_picks_a_variant():
     assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
     v, ms = g.Tuning()
     assert v in (0, 1, 2) and min(ms) > 0 and ms[v] == min(ms)
+
+
+def test_second_handle_reuses_tuning_and_pooled_memory():
+    """A fresh handle on the same mesh takes the cached autotuner decision
+    and pooled device memory, and assembles the identical matrix."""
+    c = case("grating", 2, 6.0)
+    vals, tun = [], []
+    for _ in range(2):
+        g = AsmGpuGlobal(c.prob)
+        assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
+        vals.append(g.DownloadValues())
+        tun.append(g.Tuning())
+        g.Release()
+    assert tun[0] == tun[1]
+    np.testing.assert_array_equal(vals[0], vals[1])
+    assert _lib.lib().lfasm_trim_pool(0) == 0
+    assert _lib.lib().lfasm_trim_pool(-1) == 1
