@@ -59,22 +59,26 @@ int fail(int code, const char *fmt, ...) {
 
 #define LF_LAUNCHED() g_launches.fetch_add(1, std::memory_order_relaxed)
 
-// Device memory of the handles comes from one stream-ordered pool per
-// device, owned by the library, whose release threshold keeps freed blocks:
-// the multi-GB element and value buffers of a destroyed handle are handed to
-// the next handle without a cudaMalloc/cudaFree round trip to the driver.
-// Allocations and frees are ordered on the legacy default stream;
-// lfasm_trim_pool returns the cached blocks to the driver.
+// Device memory of the handles.  Blocks of BIG_BLOCK bytes and more (the
+// element buffer, the CSR values, columns and slot maps) are cudaMalloc'd in
+// 2 MiB multiples and, when released, kept in a per-device cache keyed by
+// size: a request is served by the smallest cached block that is at least
+// as large and at most 1/8 larger, so a new handle on a mesh of the same size
+// (one handle per design iteration) gets the same blocks back without a
+// cudaMalloc/cudaFree round trip or a growing, fragmented pool.  Smaller
+// blocks come from a stream-ordered pool per device (release threshold:
+// keep everything), allocated and freed on the legacy default stream.  Every
+// release happens after the work that used the block has completed.
+// lfasm_trim_pool hands all cached memory back to the driver.
 constexpr int MAX_DEV = 64;
+constexpr size_t BIG_BLOCK = size_t(16) << 20;
+constexpr size_t BIG_ROUND = size_t(2) << 20;
 std::mutex g_pool_mu;
 cudaMemPool_t g_pool[MAX_DEV] = {};
+std::multimap<size_t, void *> g_big_free[MAX_DEV];
+std::map<void *, size_t> g_big_live[MAX_DEV];
 
-cudaError_t dev_pool(cudaMemPool_t *out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_pool_mu);
+cudaError_t dev_pool(int dev, cudaMemPool_t *out) {  // g_pool_mu held
   if (!g_pool[dev]) {
     cudaMemPoolProps pp;
     std::memset(&pp, 0, sizeof(pp));
@@ -83,7 +87,8 @@ cudaError_t dev_pool(cudaMemPool_t *out) {
     pp.location.type = cudaMemLocationTypeDevice;
     pp.location.id = dev;
     cudaMemPool_t pool = nullptr;
-    if ((e = cudaMemPoolCreate(&pool, &pp)) != cudaSuccess) return e;
+    cudaError_t e = cudaMemPoolCreate(&pool, &pp);
+    if (e != cudaSuccess) return e;
     unsigned long long keep = ~0ull;
     if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
       cudaMemPoolDestroy(pool);
@@ -95,17 +100,63 @@ cudaError_t dev_pool(cudaMemPool_t *out) {
   return cudaSuccess;
 }
 
+// frees the cached big blocks of `dev` (g_pool_mu held, dev current)
+void drop_big_cache(int dev) {
+  for (auto &kv : g_big_free[dev]) cudaFree(kv.second);
+  g_big_free[dev].clear();
+}
+
+cudaError_t dmalloc_bytes(void **out, size_t bytes) {
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (bytes < BIG_BLOCK) {
+    cudaMemPool_t pool;
+    if ((e = dev_pool(dev, &pool)) != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(out, std::max<size_t>(bytes, 1), pool, 0);
+  }
+  const size_t want = (bytes + BIG_ROUND - 1) / BIG_ROUND * BIG_ROUND;
+  auto it = g_big_free[dev].lower_bound(want);
+  if (it != g_big_free[dev].end() && it->first <= want + want / 8) {
+    *out = it->second;
+    g_big_live[dev][it->second] = it->first;
+    g_big_free[dev].erase(it);
+    return cudaSuccess;
+  }
+  e = cudaMalloc(out, want);
+  if (e == cudaErrorMemoryAllocation) {  // give the cache back and retry once
+    cudaGetLastError();
+    drop_big_cache(dev);
+    e = cudaMalloc(out, want);
+  }
+  if (e != cudaSuccess) return e;
+  g_big_live[dev][*out] = want;
+  return cudaSuccess;
+}
+
+void dfree_bytes(void *p) {
+  if (!p) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEV) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_big_live[dev].find(p);
+  if (it != g_big_live[dev].end()) {
+    g_big_free[dev].emplace(it->second, p);
+    g_big_live[dev].erase(it);
+    return;
+  }
+  cudaFreeAsync(p, 0);
+}
+
 template <typename T>
 cudaError_t dmalloc(T *&dst, size_t count) {
-  dst = nullptr;
-  cudaMemPool_t pool;
-  cudaError_t e = dev_pool(&pool);
-  if (e != cudaSuccess) return e;
   void *p = nullptr;
-  if ((e = cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, 0)) != cudaSuccess)
-    return e;
+  cudaError_t e = dmalloc_bytes(&p, std::max<size_t>(count, 1) * sizeof(T));
   dst = static_cast<T *>(p);
-  return cudaSuccess;
+  return e;
 }
 
 template <typename T>
@@ -119,7 +170,7 @@ cudaError_t upload(T *&dst, const T *src, size_t count) {
 
 template <typename T>
 void dfree(T *&p) {
-  if (p) { cudaFreeAsync((void *)p, 0); p = nullptr; }
+  if (p) { dfree_bytes((void *)p); p = nullptr; }
 }
 
 struct DevRule {
@@ -334,14 +385,43 @@ void build_tinv(double out[24]) {
   }
 }
 
-inline double pml_s_host(const PmlParams &p, double z, double *im) {
-  double d = -1.0, smax = 0.0;
-  if (z < p.z_min) { d = (p.z_min - z) / p.thick; smax = p.smax_bot; }
-  else if (z > p.z_max) { d = (z - p.z_max) / p.thick; smax = p.smax_top; }
-  if (d < 0.0) { *im = 0.0; return 1.0; }
-  if (d > 1.0) d = 1.0;
-  *im = smax * std::pow(d, p.order);
-  return 1.0;
+// index of the first i < n with bad(i), else n; scans in blocks with a
+// branch-free reduction (vectorised) and locates the index only in a block
+// that has one
+template <class F>
+size_t first_bad(size_t n, F bad) {
+  constexpr size_t B = 8192;
+  for (size_t c = 0; c < n; c += B) {
+    const size_t e = std::min(n, c + B);
+    int any = 0;
+    for (size_t i = c; i < e; ++i) any |= bad(i);
+    if (any)
+      for (size_t i = c; i < e; ++i)
+        if (bad(i)) return i;
+  }
+  return n;
+}
+
+// reference S tables depend only on p and the two rules: cached per process
+// on the exact rule contents
+struct STables {
+  std::vector<double> key, S, S_mma;
+};
+std::mutex g_stab_mu;
+std::vector<STables> g_stab;
+
+std::vector<double> rule_key(const lfasm_asm_data *ad, int ndp) {
+  std::vector<double> k = {(double)ad->p, (double)ad->nd, (double)ndp};
+  const int nd = ad->nd;
+  for (const lfasm_ref_rule *r : {&ad->rule_cc, &ad->rule_mass}) {
+    k.push_back((double)r->nq);
+    k.insert(k.end(), r->ip, r->ip + (size_t)r->nq * 3);
+    k.insert(k.end(), r->w, r->w + r->nq);
+    k.push_back(r->vshape ? 1.0 : 0.0);
+    if (r->vshape) k.insert(k.end(), r->vshape, r->vshape + (size_t)r->nq * nd * 3);
+    k.insert(k.end(), r->curl, r->curl + (size_t)r->nq * nd * 3);
+  }
+  return k;
 }
 
 }  // namespace
@@ -380,19 +460,23 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
     return fail(LFASM_ERR_ARG, "k0 and pml thickness must be positive");
   const size_t ne = ad->ne;
   const size_t nen = ne * nd;
-  for (size_t i = 0; i < nen; ++i)
-    if (ad->dof[i] < 0 || ad->dof[i] >= ad->height)
+  {
+    const int *dof = ad->dof, *attr = ad->attr, *fo = ad->fo;
+    const double *detJ = ad->detJ;
+    const unsigned hgt = (unsigned)ad->height, nreg = (unsigned)prob->n_regions;
+    size_t i = first_bad(nen, [&](size_t k) { return (int)((unsigned)dof[k] >= hgt); });
+    if (i < nen)
       return fail(LFASM_ERR_ARG, "dof[%zu] = %d out of range [0, %d)", i, ad->dof[i], ad->height);
-  for (size_t e = 0; e < ne; ++e) {
-    if (ad->attr[e] < 1 || ad->attr[e] > prob->n_regions)
-      return fail(LFASM_ERR_ARG, "attr[%zu] = %d outside 1..%d", e, ad->attr[e], prob->n_regions);
-    if (!(ad->detJ[e] > 0.0))
-      return fail(LFASM_ERR_ARG, "detJ[%zu] not positive", e);
+    const size_t ea = first_bad(ne, [&](size_t k) { return (int)((unsigned)(attr[k] - 1) >= nreg); });
+    const size_t ed = first_bad(ne, [&](size_t k) { return (int)!(detJ[k] > 0.0); });
+    if (ea < ne && ea <= ed)
+      return fail(LFASM_ERR_ARG, "attr[%zu] = %d outside 1..%d", ea, ad->attr[ea], prob->n_regions);
+    if (ed < ne) return fail(LFASM_ERR_ARG, "detJ[%zu] not positive", ed);
+    if (ad->p >= 2) {
+      i = first_bad(ne * 4, [&](size_t k) { return (int)((unsigned)fo[k] > 5u); });
+      if (i < ne * 4) return fail(LFASM_ERR_ARG, "fo[%zu] = %d outside 0..5", i, ad->fo[i]);
+    }
   }
-  if (ad->p >= 2)
-    for (size_t i = 0; i < ne * 4; ++i)
-      if (ad->fo[i] < 0 || ad->fo[i] > 5)
-        return fail(LFASM_ERR_ARG, "fo[%zu] = %d outside 0..5", i, ad->fo[i]);
 
   int ndev = 0;
   LF_CUDA(cudaGetDeviceCount(&ndev));
@@ -440,15 +524,6 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   build_tinv(tinv);
   LF_CUDA_H(cudaMemcpyToSymbol(c_tinv, tinv, sizeof(tinv)));
 
-  // packed per-element orientation and sign bits
-  std::vector<unsigned> fop(ne, 0u);
-  std::vector<unsigned long long> sm(ne, 0ull);
-  for (size_t e = 0; e < ne; ++e) {
-    if (ad->p >= 2)
-      for (int f = 0; f < 4; ++f) fop[e] |= (unsigned)ad->fo[e * 4 + f] << (8 * f);
-    for (int k = 0; k < nd; ++k)
-      if (ad->sign[e * nd + k] < 0.0) sm[e] |= 1ull << k;
-  }
   LF_CUDA_H(upload(h->dof, ad->dof, nen));
   LF_CUDA_H(upload(h->sign, ad->sign, nen));
   LF_CUDA_H(upload(h->attr, ad->attr, ne));
@@ -456,8 +531,18 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   LF_CUDA_H(upload(h->Jinv, ad->Jinv, ne * 9));
   LF_CUDA_H(upload(h->detJ, ad->detJ, ne));
   LF_CUDA_H(upload(h->v0, ad->v0, ne * 3));
-  LF_CUDA_H(upload(h->fopack, fop.data(), ne));
-  LF_CUDA_H(upload(h->signmask, sm.data(), ne));
+  // packed per-element orientation and sign bits, formed on the device
+  {
+    int *dfo = nullptr;
+    if (ad->p >= 2) LF_CUDA_H(upload(dfo, ad->fo, ne * 4));
+    LF_CUDA_H(dmalloc(h->fopack, ne));
+    LF_CUDA_H(dmalloc(h->signmask, ne));
+    k_pack<<<(unsigned)((ne + 255) / 256), 256>>>((int)ne, nd, ad->p, h->sign, dfo, h->fopack,
+                                                  h->signmask);
+    LF_LAUNCHED();
+    LF_CUDA_H(cudaGetLastError());
+    dfree(dfo);
+  }
   auto up_rule = [&](DevRule &d, const lfasm_ref_rule &r) -> cudaError_t {
     d.nq = r.nq;
     cudaError_t e;
@@ -498,35 +583,57 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   pm.smax_top = -std::log(prob->pml_target) * (prob->pml_order + 1) /
                 (2.0 * prob->k0 * n_top * prob->pml_thick);
 
-  // classify: bulk iff s(z_q) == 1 exactly at every point of both rules
-  std::vector<int> bl, pl;
-  bl.reserve(ne);
-  for (size_t e = 0; e < ne; ++e) {
-    const double *J = ad->J + e * 9;
-    const double z0 = ad->v0[e * 3 + 2];
-    bool bulk = true;
-    for (int rr = 0; rr < 2 && bulk; ++rr) {
-      const lfasm_ref_rule &R = rr == 0 ? ad->rule_cc : ad->rule_mass;
-      for (int q = 0; q < R.nq && bulk; ++q) {
-        const double z = z0 + J[6] * R.ip[q * 3] + J[7] * R.ip[q * 3 + 1] + J[8] * R.ip[q * 3 + 2];
-        double im;
-        pml_s_host(pm, z, &im);
-        if (im != 0.0 || z < pm.z_min || z > pm.z_max) bulk = false;
-      }
-    }
-    (bulk ? bl : pl).push_back((int)e);
+  // classify on the device: bulk iff s(z_q) == 1 exactly at every point of
+  // both rules; both element lists stay in ascending element order
+  std::vector<int> has_bulk(prob->n_regions, 0);
+  {
+    int *flag = nullptr, *pos = nullptr, *rhb = nullptr;
+    unsigned char *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    LF_CUDA_H(dmalloc(flag, ne + 1));
+    LF_CUDA_H(dmalloc(pos, ne + 1));
+    LF_CUDA_H(dmalloc(rhb, (size_t)prob->n_regions));
+    LF_CUDA_H(dmalloc(h->bulk_list, ne));
+    LF_CUDA_H(dmalloc(h->pml_list, ne));
+    LF_CUDA_H(cudaMemsetAsync(flag, 0, (ne + 1) * sizeof(int), 0));
+    LF_CUDA_H(cudaMemsetAsync(rhb, 0, (size_t)prob->n_regions * sizeof(int), 0));
+    const unsigned gb = (unsigned)((ne + 255) / 256);
+    k_classify<<<gb, 256>>>((int)ne, h->rcc.view(), h->rm.view(), h->J, h->v0, h->attr,
+                            pm.z_min, pm.z_max, flag, rhb);
+    LF_LAUNCHED();
+    LF_CUDA_H(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, flag, pos, (int)ne + 1, 0));
+    LF_CUDA_H(dmalloc(tmp, tmp_bytes));
+    LF_CUDA_H(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, flag, pos, (int)ne + 1, 0));
+    k_split_lists<<<gb, 256>>>((int)ne, flag, pos, h->bulk_list, h->pml_list);
+    LF_LAUNCHED();
+    int nb = 0;
+    LF_CUDA_H(cudaMemcpy(&nb, pos + ne, sizeof(int), cudaMemcpyDeviceToHost));
+    LF_CUDA_H(cudaMemcpy(has_bulk.data(), rhb, has_bulk.size() * sizeof(int),
+                         cudaMemcpyDeviceToHost));
+    dfree(flag); dfree(pos); dfree(rhb); dfree(tmp);
+    h->n_bulk = nb;
+    h->n_pml = (int)ne - nb;
   }
-  h->n_bulk = (int)bl.size();
-  h->n_pml = (int)pl.size();
-  LF_CUDA_H(upload(h->bulk_list, bl.data(), bl.size()));
-  LF_CUDA_H(upload(h->pml_list, pl.data(), pl.size()));
   if (h->n_bulk) LF_CUDA_H(dmalloc(h->rec, (size_t)h->n_bulk * REC));
 
-  std::vector<double> S;
-  build_S(ad, h->ndp, S);
-  LF_CUDA_H(upload(h->S, S.data(), S.size()));
-  build_S_mma(ad, h->ndp, S);
-  LF_CUDA_H(upload(h->S_mma, S.data(), S.size()));
+  {
+    std::vector<double> key = rule_key(ad, h->ndp);
+    std::lock_guard<std::mutex> lk(g_stab_mu);
+    const STables *hit = nullptr;
+    for (const STables &t : g_stab)
+      if (t.key == key) { hit = &t; break; }
+    if (!hit) {
+      STables t;
+      t.key = std::move(key);
+      build_S(ad, h->ndp, t.S);
+      build_S_mma(ad, h->ndp, t.S_mma);
+      if (g_stab.size() >= 16) g_stab.erase(g_stab.begin());
+      g_stab.push_back(std::move(t));
+      hit = &g_stab.back();
+    }
+    LF_CUDA_H(upload(h->S, hit->S.data(), hit->S.size()));
+    LF_CUDA_H(upload(h->S_mma, hit->S_mma.data(), hit->S_mma.size()));
+  }
   if (h->n_bulk)
     LF_CUDA_H(dmalloc(h->rec_mma, (size_t)h->n_bulk * BREC));
 
@@ -566,7 +673,9 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
       }
     }
     h->n_src = (int)src.size();
-    for (int e : bl) h->max_bulk_slab = std::max(h->max_bulk_slab, slab[e]);
+    for (int r = 0; r < prob->n_regions; ++r)
+      if (has_bulk[r])
+        h->max_bulk_slab = std::max(h->max_bulk_slab, prob->region_slab ? prob->region_slab[r] : 0);
     LF_CUDA_H(upload(h->slab_of, slab.data(), ne));
     LF_CUDA_H(upload(h->delta, del.data(), ne));
     LF_CUDA_H(upload(h->src_list, src.data(), src.size()));
@@ -1323,17 +1432,19 @@ void lfasm_destroy(lfasm_handle *h) {
 
 int lfasm_trim_pool(int gpu_id) {
   if (gpu_id < 0 || gpu_id >= MAX_DEV) return fail(LFASM_ERR_ARG, "gpu_id %d out of range", gpu_id);
-  cudaMemPool_t pool = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    pool = g_pool[gpu_id];
-  }
-  if (!pool) return LFASM_OK;
   int cur = 0;
   LF_CUDA(cudaGetDevice(&cur));
-  LF_CUDA(cudaSetDevice(gpu_id));
-  cudaError_t e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  cudaError_t e = cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[gpu_id] && g_big_free[gpu_id].empty()) return LFASM_OK;
+    e = cudaSetDevice(gpu_id);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) {
+      drop_big_cache(gpu_id);
+      if (g_pool[gpu_id]) e = cudaMemPoolTrimTo(g_pool[gpu_id], 0);
+    }
+  }
   cudaSetDevice(cur);
   LF_CUDA(e);
   return LFASM_OK;

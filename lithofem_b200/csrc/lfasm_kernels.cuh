@@ -895,6 +895,73 @@ __global__ void k_max_reduce(int n, const int *__restrict__ ptr, int diff, int *
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Warp-wide bitonic sort of 32 K ints held in registers, element i at
+// x[i >> 5] of lane i & 31: partners closer than 32 are exchanged by
+// shuffles, farther ones are register swaps inside a lane.
+template <int K>
+__device__ __forceinline__ void warp_sort_reg(int (&x)[K], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * K; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int J = j >> 5;
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+          if ((s & J) == 0) {
+            const bool up = ((s << 5) & k) == 0;
+            const int a = x[s], b = x[s | J];
+            const int lo = min(a, b), hi = max(a, b);
+            x[s] = up ? lo : hi;
+            x[s | J] = up ? hi : lo;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+          const bool up = (((s << 5) | lane) & k) == 0;
+          const int v = x[s];
+          const int o = __shfl_xor_sync(0xffffffffu, v, j);
+          x[s] = (((lane & j) == 0) == up) ? min(v, o) : max(v, o);
+        }
+      }
+    }
+  }
+}
+
+// the row's candidate columns (sentinel-padded to 32 K), sorted in registers
+// and compacted to the unique list in buf; returns its length
+template <int K>
+__device__ __forceinline__ int row_unique_reg(const int *lst, int tot, int nd,
+                                              const int *__restrict__ dof, int *buf, int lane) {
+  int x[K];
+#pragma unroll
+  for (int s = 0; s < K; ++s) {
+    const int i = (s << 5) | lane;
+    int v = 0x7fffffff;
+    if (i < tot) {
+      const int id = lst[i / nd];
+      v = dof[(size_t)(id / nd) * nd + (i % nd)];
+    }
+    x[s] = v;
+  }
+  warp_sort_reg<K>(x, lane);
+  int nr = 0, last = -1;
+#pragma unroll
+  for (int s = 0; s < K; ++s) {
+    const int v = x[s];
+    int prev = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) prev = last;
+    last = __shfl_sync(0xffffffffu, v, 31);
+    const bool keep = v != 0x7fffffff && v != prev;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) buf[nr + __popc(bal & ((1u << lane) - 1u))] = v;
+    nr += __popc(bal);
+  }
+  __syncwarp();
+  return nr;
+}
+
 // one warp per row.  Both passes first sort the row's (element, row) list
 // (the gather sums in that order).
 // PASS 1: sort the candidate columns (every dof of every listed element),
@@ -949,40 +1016,52 @@ __global__ void k_row_symbolic(int n, int nd, const int *__restrict__ dof,
   }
   int len = 32;  // this row's sort length; tot <= cap
   while (len < tot) len <<= 1;
-  for (int i = lane; i < len; i += 32) {
-    int v = 0x7fffffff;
-    if (i < tot) {
-      const int id = lst[i / nd];
-      v = dof[(size_t)(id / nd) * nd + (i % nd)];
+  int nr = 0;
+  if (len <= 1024) {
+    switch (len) {
+      case 32: nr = row_unique_reg<1>(lst, tot, nd, dof, buf, lane); break;
+      case 64: nr = row_unique_reg<2>(lst, tot, nd, dof, buf, lane); break;
+      case 128: nr = row_unique_reg<4>(lst, tot, nd, dof, buf, lane); break;
+      case 256: nr = row_unique_reg<8>(lst, tot, nd, dof, buf, lane); break;
+      case 512: nr = row_unique_reg<16>(lst, tot, nd, dof, buf, lane); break;
+      default: nr = row_unique_reg<32>(lst, tot, nd, dof, buf, lane); break;
     }
-    buf[i] = v;
-  }
-  __syncwarp();
-  // bitonic sort (ascending); each lane takes compare pairs (i, i | j)
-  for (int k = 2; k <= len; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int pi = lane; pi < (len >> 1); pi += 32) {
-        const int i = ((pi & ~(j - 1)) << 1) | (pi & (j - 1));
-        const int ixj = i | j;
-        const int a = buf[i], b = buf[ixj];
-        if ((a > b) == ((i & k) == 0)) { buf[i] = b; buf[ixj] = a; }
+  } else {
+    for (int i = lane; i < len; i += 32) {
+      int v = 0x7fffffff;
+      if (i < tot) {
+        const int id = lst[i / nd];
+        v = dof[(size_t)(id / nd) * nd + (i % nd)];
       }
+      buf[i] = v;
+    }
+    __syncwarp();
+    // bitonic sort (ascending); each lane takes compare pairs (i, i | j)
+    for (int k = 2; k <= len; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int pi = lane; pi < (len >> 1); pi += 32) {
+          const int i = ((pi & ~(j - 1)) << 1) | (pi & (j - 1));
+          const int ixj = i | j;
+          const int a = buf[i], b = buf[ixj];
+          if ((a > b) == ((i & k) == 0)) { buf[i] = b; buf[ixj] = a; }
+        }
+        __syncwarp();
+      }
+    }
+    // unique, compacted in place (a chunk writes only at or below what it read)
+    int last = -1;
+    for (int c0 = 0; c0 < len; c0 += 32) {
+      const int v = buf[c0 + lane];
+      int prev = __shfl_up_sync(0xffffffffu, v, 1);
+      if (lane == 0) prev = last;
+      last = __shfl_sync(0xffffffffu, v, 31);
+      const bool keep = v != 0x7fffffff && v != prev;
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      __syncwarp();
+      if (keep) buf[nr + __popc(bal & ((1u << lane) - 1u))] = v;
+      nr += __popc(bal);
       __syncwarp();
     }
-  }
-  // unique, compacted in place (a chunk writes only at or below what it read)
-  int nr = 0, last = -1;
-  for (int c0 = 0; c0 < len; c0 += 32) {
-    const int v = buf[c0 + lane];
-    int prev = __shfl_up_sync(0xffffffffu, v, 1);
-    if (lane == 0) prev = last;
-    last = __shfl_sync(0xffffffffu, v, 31);
-    const bool keep = v != 0x7fffffff && v != prev;
-    const unsigned bal = __ballot_sync(0xffffffffu, keep);
-    __syncwarp();
-    if (keep) buf[nr + __popc(bal & ((1u << lane) - 1u))] = v;
-    nr += __popc(bal);
-    __syncwarp();
   }
   if (lane == 0) cnt[r] = nr;
   int *dst = tmpJ + (size_t)p0 * nd;
@@ -1011,6 +1090,63 @@ __global__ void k_row_compact(int n, int nd, const int *__restrict__ ea_ptr,
   const int *src = tmpJ + (size_t)ea_ptr[r] * nd;
   const int rb = I[r], len = I[r + 1] - rb;
   for (int j = lane; j < len; j += 32) Jc[rb + j] = src[j];
+}
+
+// ---------------------------------------------------------------------------
+// init-time passes over the uploaded element arrays
+// ---------------------------------------------------------------------------
+// per element: the four face orientation codes in one word (8 bits each)
+// and the dof sign bits
+__global__ void k_pack(int ne, int nd, int p, const double *__restrict__ sign,
+                       const int *__restrict__ fo, unsigned *__restrict__ fopack,
+                       unsigned long long *__restrict__ signmask) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  unsigned f = 0u;
+  if (p >= 2)
+    for (int k = 0; k < 4; ++k) f |= (unsigned)fo[(size_t)e * 4 + k] << (8 * k);
+  unsigned long long m = 0ull;
+  for (int k = 0; k < nd; ++k)
+    if (sign[(size_t)e * nd + k] < 0.0) m |= 1ull << k;
+  fopack[e] = f;
+  signmask[e] = m;
+}
+
+// bulk iff every quadrature point of both rules has z_min <= z <= z_max
+// (the stretch is then exactly 1); z is formed with explicit roundings, in
+// the order z0 + J20 x + J21 y + J22 z, so that the result does not depend on
+// multiply-add contraction.  flag[e] = 1 for bulk; region_has_bulk marks the
+// regions that own a bulk element.
+__global__ void k_classify(int ne, Rule rcc, Rule rm, const double *__restrict__ J9,
+                           const double *__restrict__ v0, const int *__restrict__ attr,
+                           double z_min, double z_max, int *__restrict__ flag,
+                           int *__restrict__ region_has_bulk) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const double z0 = v0[(size_t)e * 3 + 2];
+  const double a = J9[(size_t)e * 9 + 6], b = J9[(size_t)e * 9 + 7], c = J9[(size_t)e * 9 + 8];
+  bool bulk = true;
+  for (int rr = 0; rr < 2 && bulk; ++rr) {
+    const Rule &R = rr == 0 ? rcc : rm;
+    for (int q = 0; q < R.nq && bulk; ++q) {
+      const double z = __dadd_rn(__dadd_rn(__dadd_rn(z0, __dmul_rn(a, R.ip[q * 3])),
+                                           __dmul_rn(b, R.ip[q * 3 + 1])),
+                                 __dmul_rn(c, R.ip[q * 3 + 2]));
+      if (z < z_min || z > z_max) bulk = false;
+    }
+  }
+  flag[e] = bulk ? 1 : 0;
+  if (bulk) region_has_bulk[attr[e] - 1] = 1;
+}
+
+// ordered split of 0..ne-1 into the bulk and PML lists from the exclusive
+// scan of the bulk flags
+__global__ void k_split_lists(int ne, const int *__restrict__ flag, const int *__restrict__ pos,
+                              int *__restrict__ bulk_list, int *__restrict__ pml_list) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  if (flag[e]) bulk_list[pos[e]] = e;
+  else pml_list[e - pos[e]] = e;
 }
 
 __global__ void k_essmask(int ne, int nd, const int *__restrict__ dof,

@@ -43,3 +43,45 @@ def test_argument_validation_precedes_device_use():
     m.ad.dof = keep.ctypes.data_as(_abi.c_int_p)
     rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
     assert rc == 1 and b"out of range" in _lib.lib().lfasm_last_error()
+
+
+def _init_with(c, **arrays):
+    m = _abi.marshal(c.ad, c.prob)
+    keep = []
+    for name, arr in arrays.items():
+        a = np.ascontiguousarray(arr)
+        keep.append(a)
+        ptr_t = _abi.c_int_p if a.dtype == np.int32 else _abi.c_double_p
+        setattr(m.ad, name, a.ctypes.data_as(ptr_t))
+    h = ct.c_void_p()
+    rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
+    return rc, _lib.lib().lfasm_last_error().decode()
+
+
+def test_validation_reports_the_first_offending_entry():
+    """Each check names the lowest bad index, checks run in the order dof,
+    then per element attr before detJ, then face orientations -- all before
+    any device call."""
+    c = configs.small_case("grating", 2, 6.0)
+    dof = c.ad.dof.astype(np.int32).copy()
+    dof[[40000 % dof.size, 9000 % dof.size, 77]] = -3
+    rc, msg = _init_with(c, dof=dof)
+    assert rc == 1 and msg.startswith("dof[77] = -3 out of range")
+    attr = c.ad.attr.astype(np.int32).copy()
+    attr[[50, 20]] = len(c.prob.regions) + 1
+    detJ = c.ad.detJ.copy()
+    detJ[[30, 7]] = [np.nan, -1.0]
+    rc, msg = _init_with(c, attr=attr)
+    assert rc == 1 and msg.startswith("attr[20] =")
+    rc, msg = _init_with(c, detJ=detJ)
+    assert rc == 1 and msg == "detJ[7] not positive"
+    rc, msg = _init_with(c, attr=attr, detJ=detJ)   # element 7 is checked before 20
+    assert rc == 1 and msg == "detJ[7] not positive"
+    attr2 = attr.copy()
+    attr2[7] = 0
+    rc, msg = _init_with(c, attr=attr2, detJ=detJ)  # attr before detJ on one element
+    assert rc == 1 and msg.startswith("attr[7] = 0")
+    fo = c.ad.fo.astype(np.int32).copy()
+    fo[[11, 3]] = [6, -1]
+    rc, msg = _init_with(c, fo=fo)
+    assert rc == 1 and msg == "fo[3] = -1 outside 0..5"

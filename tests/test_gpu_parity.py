@@ -253,6 +253,33 @@ def test_autotuner_picks_a_variant():
     assert v in (0, 1, 2) and min(ms) > 0 and ms[v] == min(ms)
 
 
+def test_high_valence_row():
+    """One dof shared by 30 p=3 elements: its row has 30 x 45 candidate
+    columns, beyond the register sort (1024), so the device CSR build takes
+    its shared-memory sort; sparsity and values still match the oracle."""
+    c = case("grating", 3, 6.0)
+    ad = copy.copy(c.ad)
+    dof = ad.dof.copy().reshape(ad.ne, ad.nd)
+    x = int(dof[0, 0])
+    moved = 0
+    for e in range(1, ad.ne):
+        if moved == 29:
+            break
+        if x not in dof[e]:
+            dof[e, 0] = x
+            moved += 1
+    assert moved == 29
+    ad.dof = dof.reshape(-1)
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(ad, 0) and g.BuildGlobal(ad.ess)
+    I, J = g.DownloadCsr()
+    Io, Jo = oracle.csr(ad)
+    assert np.array_equal(I, Io) and np.array_equal(J, Jo)
+    assert Io[x + 1] - Io[x] > 1024 // 2
+    assert g.Assemble(True)
+    assert rel(g.DownloadValues(), oracle.assemble(ad, c.prob, Io, Jo, ad.ess, True)) < TOL
+
+
 def test_second_handle_reuses_tuning_and_pooled_memory():
     """A fresh handle on the same mesh takes the cached autotuner decision
     and pooled device memory, and assembles the identical matrix."""
