@@ -205,6 +205,7 @@ struct lfasm_handle {
   double *rec = nullptr;
   // tensor-core bulk variant and the autotuned choice
   double *S_mma = nullptr, *rec_mma = nullptr;
+  double *S_mmaf = nullptr;  // B operand of the fused Bloch layout
   int bulk_variant = 0;      // 0: k_bulk (SIMT), 1/2: k_bulk_mma (DMMA, 4/2 tiles per warp)
   int tuned = 0;             // autotune done
   int forced = 0;            // variant fixed by lfasm_set_bulk_variant
@@ -315,7 +316,9 @@ void build_S(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
 // 6..11 Svv (symmetric pairs), 12..20 Rvc_jj', 21..29 Rcv_jj'.
 int bulk_tiles(int ndp) { return 2 * (ndp / 2) * ((ndp + 7) / 8); }
 
-void build_S_mma(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
+// fused: the fused Bloch layout of k_bulk_mma<..., FUSED> -- terms 0..11 as
+// above, 12..17 Svv again (imaginary row), 18..26 D_ab = Rvc_ab - Rcv_ba.
+void build_S_mma(const lfasm_asm_data *ad, int ndp, bool fused, std::vector<double> &S) {
   const int nd = ad->nd;
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
   const lfasm_ref_rule &rc = ad->rule_cc, &rm = ad->rule_mass;
@@ -361,9 +364,17 @@ void build_S_mma(const lfasm_asm_data *ad, int ndp, std::vector<double> &S) {
             S[(size_t)(6 + t) * N + n] = x == y ? at(Rvv, x * 3 + x, k, l)
                                                 : at(Rvv, x * 3 + y, k, l) + at(Rvv, y * 3 + x, k, l);
           }
-          for (int j = 0; j < 9; ++j) {
-            S[(size_t)(12 + j) * N + n] = at(Rvc, j, k, l);
-            S[(size_t)(21 + j) * N + n] = at(Rcv, j, k, l);
+          if (fused) {
+            for (int t = 0; t < 6; ++t) S[(size_t)(12 + t) * N + n] = S[(size_t)(6 + t) * N + n];
+            for (int a2 = 0; a2 < 3; ++a2)
+              for (int b2 = 0; b2 < 3; ++b2)
+                S[(size_t)(18 + a2 * 3 + b2) * N + n] =
+                    at(Rvc, a2 * 3 + b2, k, l) - at(Rcv, b2 * 3 + a2, k, l);
+          } else {
+            for (int j = 0; j < 9; ++j) {
+              S[(size_t)(12 + j) * N + n] = at(Rvc, j, k, l);
+              S[(size_t)(21 + j) * N + n] = at(Rcv, j, k, l);
+            }
           }
         }
 }
@@ -405,7 +416,7 @@ size_t first_bad(size_t n, F bad) {
 // reference S tables depend only on p and the two rules: cached per process
 // on the exact rule contents
 struct STables {
-  std::vector<double> key, S, S_mma;
+  std::vector<double> key, S, S_mma, S_mmaf;
 };
 std::mutex g_stab_mu;
 std::vector<STables> g_stab;
@@ -626,13 +637,15 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
       STables t;
       t.key = std::move(key);
       build_S(ad, h->ndp, t.S);
-      build_S_mma(ad, h->ndp, t.S_mma);
+      build_S_mma(ad, h->ndp, false, t.S_mma);
+      build_S_mma(ad, h->ndp, true, t.S_mmaf);
       if (g_stab.size() >= 16) g_stab.erase(g_stab.begin());
       g_stab.push_back(std::move(t));
       hit = &g_stab.back();
     }
     LF_CUDA_H(upload(h->S, hit->S.data(), hit->S.size()));
     LF_CUDA_H(upload(h->S_mma, hit->S_mma.data(), hit->S_mma.size()));
+    LF_CUDA_H(upload(h->S_mmaf, hit->S_mmaf.data(), hit->S_mmaf.size()));
   }
   if (h->n_bulk)
     LF_CUDA_H(dmalloc(h->rec_mma, (size_t)h->n_bulk * BREC));
@@ -783,10 +796,12 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     LF_LAUNCHED();
   } else if (h->n_bulk) {
     const int nb = h->n_bulk;
+    // both cross terms or neither: the fused Bloch layout (7 k-steps a tile)
+    const bool fused = ((mask & LFASM_CROSS0) != 0) == ((mask & LFASM_CROSS1) != 0);
     k_prep_bulk_mma<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, h->bulk_list, h->J, h->Jinv,
                                                              h->detJ, h->attr, h->eps_tab,
                                                              h->elem_eps, h->pml, mask,
-                                                             h->rec_mma);
+                                                             fused ? 1 : 0, h->rec_mma);
     LF_LAUNCHED();
     const int ntiles = bulk_tiles(h->ndp);
     const int TT = h->bulk_variant == 1 ? 4 : 2;  // tiles per warp
@@ -797,17 +812,21 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     const long long want = (long long)h->sm_count * 8;
     const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
     dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
-#define LF_BULKM(C, M, T)                                                         \
-  k_bulk_mma<C, M, T><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                   \
-      nb, h->bulk_list, h->rec_mma, h->S_mma, ntiles, h->nd, h->ndp, h->p, bchunk, \
-      te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
+#define LF_BULKM(C, M, T, F)                                                      \
+  k_bulk_mma<C, M, T, F><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                \
+      nb, h->bulk_list, h->rec_mma, F ? h->S_mmaf : h->S_mma, ntiles, h->nd, h->ndp, \
+      h->p, bchunk, te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
+#define LF_BULKM_T(T, F)                                                          \
+  do {                                                                            \
+    if (cross) { if (mode) LF_BULKM(true, 1, T, F); else LF_BULKM(true, 0, T, F); }   \
+    else { if (mode) LF_BULKM(false, 1, T, F); else LF_BULKM(false, 0, T, F); }       \
+  } while (0)
     if (TT == 4) {
-      if (cross) { if (mode) LF_BULKM(true, 1, 4); else LF_BULKM(true, 0, 4); }
-      else { if (mode) LF_BULKM(false, 1, 4); else LF_BULKM(false, 0, 4); }
+      if (fused) LF_BULKM_T(4, true); else LF_BULKM_T(4, false);
     } else {
-      if (cross) { if (mode) LF_BULKM(true, 1, 2); else LF_BULKM(true, 0, 2); }
-      else { if (mode) LF_BULKM(false, 1, 2); else LF_BULKM(false, 0, 2); }
+      if (fused) LF_BULKM_T(2, true); else LF_BULKM_T(2, false);
     }
+#undef LF_BULKM_T
 #undef LF_BULKM
     LF_LAUNCHED();
   }
@@ -1418,7 +1437,7 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
   for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
-  dfree(h->S); dfree(h->rec); dfree(h->S_mma); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
+  dfree(h->S); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
   dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->off); dfree(h->partials);
   dfree(h->red);

@@ -339,12 +339,54 @@ constexpr int BREC = 2 * BK;    // doubles per element record: real row, imagina
 constexpr int BULK_T = 4;       // N tiles (8 entries) per warp
 constexpr int BULK_WARPS = 4;
 
+// One coefficient row of 32 terms for the fused Bloch layout (both cross
+// terms on, or neither): [0..5] curl-curl and [6..11] mass+KLK real parts at
+// the symmetric pairs, [12..17] mass imaginary parts, [18..26] G^vc =
+// Jinv K J.  Because K is antisymmetric, G^cv = J^T K Jinv^T = -(G^vc)^T,
+// so the two cross terms i(G^vc : R^vc + G^cv : R^cv) collapse onto
+// G^vc : D with D_ab = R^vc_ab - R^cv_ba (a table column of the B operand).
+__device__ __forceinline__ void bulk_record_fused(const double *J, const double *Ji, double det,
+                                                  double me_re, double me_im, const double *K,
+                                                  const double *mKK, bool cc, bool ms,
+                                                  bool cross, bool kl, double *r) {
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  for (int t = 0; t < BK; ++t) r[t] = 0.0;
+  for (int t = 0; t < 6; ++t) {
+    const int a = pa[t], b = pb[t];
+    if (cc) r[t] = (J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b]) / det;
+    const double jj = Ji[a * 3 + 0] * Ji[b * 3 + 0] + Ji[a * 3 + 1] * Ji[b * 3 + 1] +
+                      Ji[a * 3 + 2] * Ji[b * 3 + 2];
+    double vr = 0.0, vi = 0.0;
+    if (ms) { vr += me_re * jj; vi += me_im * jj; }
+    if (kl) {
+      double s = 0.0;
+      for (int rr = 0; rr < 3; ++rr)
+        for (int c2 = 0; c2 < 3; ++c2) s += Ji[a * 3 + rr] * mKK[rr * 3 + c2] * Ji[b * 3 + c2];
+      vr += s;
+    }
+    r[6 + t] = det * vr;
+    r[12 + t] = det * vi;
+  }
+  if (cross)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double gvc = 0.0;
+        for (int rr = 0; rr < 3; ++rr)
+          for (int c2 = 0; c2 < 3; ++c2) {
+            const double k = K[rr * 3 + c2];
+            if (k == 0.0) continue;
+            gvc += Ji[a * 3 + rr] * k * J[c2 * 3 + b];
+          }
+        r[18 + a * 3 + b] = gvc;
+      }
+}
+
 __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
                             const double *__restrict__ J9, const double *__restrict__ Ji9,
                             const double *__restrict__ detJ, const int *__restrict__ attr,
                             const dcplx *__restrict__ eps_tab,
                             const dcplx *__restrict__ elem_eps, PmlParams pml,
-                            int mask, double *__restrict__ rec) {
+                            int mask, int fused, double *__restrict__ rec) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nb) return;
   const int e = list[i];
@@ -366,6 +408,11 @@ __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
   const double mKK[9] = {ky * ky, -kx * ky, 0.0, -kx * ky, kx * kx, 0.0, 0.0, 0.0,
                          kx * kx + ky * ky};
   const double me_re = -k2 * eps.re, me_im = -k2 * eps.im;
+  if (fused) {
+    bulk_record_fused(J, Ji, det, me_re, me_im, K, mKK, cc, ms, c0 && c1, kl,
+                      rec + (size_t)i * BK);
+    return;
+  }
   for (int t = 0; t < BK; ++t) { re[t] = 0.0; im[t] = 0.0; }
   for (int t = 0; t < 6; ++t) {
     const int a = pa[t], b = pb[t];
@@ -403,7 +450,11 @@ __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
 // element is one full 128-byte line of the (row-padded) element matrix.  A
 // warp owns BULK_T/2 row-pair blocks (I, cb), i.e. both rows of each pair:
 // the row transform is thread-local, the column pair is thread-local.
-template <bool CROSS, int MODE, int TT>
+// FUSED: the fused Bloch layout (one 32-term coefficient row per element,
+// real part from k-steps 0..2, imaginary part from 3..4, or 3..6 with the
+// cross terms); otherwise the general layout (a real row and an imaginary
+// row of 32 terms, k-steps 0..2 and 1..7).
+template <bool CROSS, int MODE, int TT, bool FUSED>
 __global__ void __launch_bounds__(BULK_WARPS * 32)
 k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
            const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
@@ -416,7 +467,8 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   __shared__ unsigned sfo[8];
   __shared__ unsigned long long ssm[8], sem[8];
   constexpr int PB = TT / 2;               // row-pair blocks per warp
-  constexpr int KS = BK / 4;
+  constexpr int KS = FUSED ? 7 : BK / 4;   // B k-steps held in registers
+  constexpr int RECW = FUSED ? BK : BREC;  // doubles per element record
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int g = lane >> 2, t4 = lane & 3;
   const int ncb = (ndp + 7) / 8;           // column blocks of 8
@@ -447,7 +499,7 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
   const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
   // the next batch's records and element metadata are loaded into registers
   // while the current batch is computed
-  constexpr int PF = (8 * BREC + BULK_WARPS * 32 - 1) / (BULK_WARPS * 32);
+  constexpr int PF = (8 * RECW + BULK_WARPS * 32 - 1) / (BULK_WARPS * 32);
   double pf[PF];
   int pfe = -1;
   unsigned pfo = 0u;
@@ -458,7 +510,7 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int j = tid + u * BULK_WARPS * 32;
-      pf[u] = (j < 8 * BREC && (j / BREC) < nel) ? rec[(size_t)ebase * BREC + j] : 0.0;
+      pf[u] = (j < 8 * RECW && (j / RECW) < nel) ? rec[(size_t)ebase * RECW + j] : 0.0;
     }
     pfe = tid < nel ? list[ebase + tid] : -1;
     if (pfe >= 0) {
@@ -473,7 +525,7 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 #pragma unroll
     for (int u = 0; u < PF; ++u) {
       const int j = tid + u * BULK_WARPS * 32;
-      if (j < 8 * BREC) sA[j] = pf[u];
+      if (j < 8 * RECW) sA[j] = pf[u];
     }
     if (tid < 8) {
       se[tid] = pfe;
@@ -485,9 +537,10 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
     prefetch(bt + 1);
     double ar[3], ai[KS];
 #pragma unroll
-    for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * BREC + ks * 4 + t4];
+    for (int ks = 0; ks < 3; ++ks) ar[ks] = sA[g * RECW + ks * 4 + t4];
 #pragma unroll
-    for (int ks = 0; ks < KS; ++ks) ai[ks] = sA[g * BREC + BK + ks * 4 + t4];
+    for (int ks = 0; ks < KS; ++ks)
+      ai[ks] = FUSED ? (ks >= 3 ? sA[g * RECW + ks * 4 + t4] : 0.0) : sA[g * RECW + BK + ks * 4 + t4];
     const int e = se[g];
     const unsigned fp = sfo[g];
     const unsigned long long sm = ssm[g], em = sem[g];
@@ -501,8 +554,13 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
         cr[a][0] = cr[a][1] = ci[a][0] = ci[a][1] = 0.0;
 #pragma unroll
         for (int ks = 0; ks < 3; ++ks) dmma(cr[a][0], cr[a][1], ar[ks], bf[j][a][ks]);
+        if (FUSED) {
 #pragma unroll
-        for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
+          for (int ks = 3; ks < (CROSS ? 7 : 5); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
+        } else {
+#pragma unroll
+          for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
+        }
       }
       if (!okv[j] || e < 0) continue;
       if (fcv[j] >= 0) {  // columns: A <- A M
@@ -580,7 +638,10 @@ template <int NDP8>
 struct PmlShape {
   static constexpr int NW = NDP8 / 8;                    // warps = column tiles
   static constexpr int MT = NDP8 / 8;                    // row tiles
-  static constexpr int LD = (NDP8 % 16 == 0) ? NDP8 + 8 : NDP8;  // row stride = 8 mod 16
+  // row stride = 4 mod 16 doubles: the fragment loads of one DMMA (lane
+  // (g, t4) reads row r0 + t4, column 8 m + g) then fall on 16 distinct
+  // 8-byte bank pairs in each half-warp
+  static constexpr int LD = NDP8 + ((4 - NDP8 % 16) + 16) % 16;
   static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
   static constexpr size_t SMEM =
       (size_t)3 * RMAX * LD * sizeof(double) + PML_MAXQ * sizeof(QCoef);
