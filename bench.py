@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--config", type=int, default=3,
+                    help="1-4: one mesh; 5: the 16 polygon-hole meshes in one CUDA-graph launch")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -215,6 +216,10 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if a.config == 5:
+        if a.impl == "reference":
+            return run_reference_batch(a, rank, world, dist)
+        return run_batch(a, rank, world, local, dist, torch)
     if a.impl == "reference":
         return run_reference(a, rank, world, dist)
     return run_ours(a, rank, world, local, dist, torch)
@@ -478,6 +483,235 @@ def run_e2e(a, case, dev, torch, stream) -> dict | None:
             "timer": "host wall clock with device synchronize on both sides",
             "breakdown_ms": {"init": br[0], "build_global": br[1], "assemble": br[2],
                              "d2h": br[3], "release": br[4]}}
+
+
+def batch_workload_config(cases, a) -> dict:
+    return {"workload": f"C5 batched uneven meshes: {len(cases)} polygon holes, p = 1, 2, 3 "
+                        f"cycled, {min(c.ad.height for c in cases) / 1e3:.0f}k-"
+                        f"{max(c.ad.height for c in cases) / 1e3:.0f}k DOF, one CUDA-graph launch",
+            "meshes": [{"name": c.name, "p": c.p, "elements": c.ad.ne, "ndof": c.ad.height,
+                        "nnz": int(getattr(c, "nnz", 0))} for c in cases],
+            "ndof": int(sum(c.ad.height for c in cases)),
+            "nnz": int(sum(getattr(c, "nnz", 0) for c in cases)),
+            "l2_policy": "inputs larger than L2 (element buffers and CSR >> 126 MB)",
+            "replicas": a.gpus, "scale": a.scale}
+
+
+def run_batch(a, rank, world, local, dist, torch):
+    """The batched workload: 16 polygon-hole meshes assembled by one graph
+    launch (lfasm_batch_assemble); value = total nnz / time per launch."""
+    from lithofem_b200 import _lib, configs
+    from lithofem_b200.asm import AsmBatch, AsmGpuGlobal
+    dev = local
+    torch.cuda.set_device(dev)
+    cases = configs.batch_config(scale=a.scale)
+    stream = torch.cuda.current_stream()
+    hs = []
+    for c in cases:
+        g = AsmGpuGlobal(c.prob)
+        assert g.Init(c.ad, dev) and g.BuildGlobal(c.ad.ess)
+        c.nnz = g.nnz()
+        hs.append(g)
+    total = sum(c.nnz for c in cases)
+    # per-mesh stage profile (serial, untimed) and the serial per-handle time
+    stages = np.zeros(3)
+    serial_ms = 0.0
+    for g in hs:
+        assert g.Assemble(True)          # tunes the handle
+        assert g.SetProfile(True)
+        assert g.Assemble(True)
+        st = np.array(g.StageTimes())
+        stages += st
+        serial_ms += float(st.sum())
+        assert g.SetProfile(False)
+    b = AsmBatch(hs)
+    assert b.SetStream(stream.cuda_stream)
+    for _ in range(a.warmup):
+        assert b.Assemble(True)
+    torch.cuda.synchronize()
+    clk = ClockSampler(dev)
+    if dist is not None:
+        dist.barrier()
+    clk.start()
+    launches0 = _lib.lib().lfasm_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        assert b.Assemble(True)
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = _lib.lib().lfasm_launch_count() - launches0
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1) / a.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = total * world / (ms * 1e-3)
+    b.Release()
+    for g in hs:
+        g.Release()
+    e2e = run_batch_e2e(a, cases, dev, torch)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    fp64 = fp64_peak_tflops(torch)
+    kern = {nm: {"ms": float(t)} for nm, t in zip(["prep+bulk", "pml", "gather"], stages)}
+    gb = sum(c.ad.ne * c.ad.nd * c.ad.nd * 18 + c.ad.ne * c.ad.nd * 4 + (c.ad.height + 1) * 8
+             + c.nnz * 16 for c in cases)
+    kern["gather"]["GB/s"] = gb / (stages[2] * 1e-3) / 1e9
+    flops = 0.0
+    for c in cases:
+        rows = 3 * c.ad.rule_cc.nq + (6 if c.prob.has_kpar else 3) * c.ad.rule_mass.nq
+        flops += float(np.sum(_pml_mask(c))) * 4.0 * rows * c.ad.nd ** 2
+    kern["pml"]["TFLOP/s"] = flops / (stages[1] * 1e-3) / 1e12 if stages[1] > 0 else 0.0
+    top = int(np.argmax(stages))
+    if top == 1:
+        roof = {"kernel": "k_pml_mma", "bound": "tensor", "achieved": kern["pml"]["TFLOP/s"],
+                "peak": fp64, "unit": "TFLOP/s", "frac": kern["pml"]["TFLOP/s"] / fp64,
+                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3", "traffic": None}
+    else:
+        nm = "gather" if top == 2 else "prep+bulk"
+        if nm == "prep+bulk":
+            bb = sum(float(np.sum(~_pml_mask(c))) * (c.ad.nd ** 2 * 16 + 256) for c in cases)
+            kern[nm]["GB/s"] = bb / (stages[0] * 1e-3) / 1e9
+        roof = {"kernel": {"gather": "k_gather", "prep+bulk": "k_bulk_mma"}[nm], "bound": "hbm",
+                "achieved": kern[nm]["GB/s"], "peak": hbm, "unit": "GB/s",
+                "frac": kern[nm]["GB/s"] / hbm,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
+    roof["what"] = "stage times summed over the 16 meshes (serial profile pass)"
+    cpu = None
+    if not a.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline_batch(cases, a.cpu_seconds, 1)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
+            "config": batch_workload_config(cases, a), "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
+            "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
+            "serial_per_handle_ms": serial_ms}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _pml_mask(c) -> np.ndarray:
+    """Elements with a quadrature point in the PML (the classification of the
+    library: z outside [z_min, z_max] at any point of either rule)."""
+    ad, prob = c.ad, c.prob
+    J = ad.J.reshape(ad.ne, 3, 3)
+    z0 = ad.v0.reshape(ad.ne, 3)[:, 2]
+    out = np.zeros(ad.ne, dtype=bool)
+    for r in (ad.rule_cc, ad.rule_mass):
+        z = z0[:, None] + J[:, 2, :] @ np.asarray(r.ip).reshape(-1, 3).T
+        out |= ((z < prob.z_min) | (z > prob.z_max)).any(axis=1)
+    return out
+
+
+def run_batch_e2e(a, cases, dev, torch) -> dict | None:
+    """e2e of the batch: every mesh's lfasm_init from pinned host arrays +
+    lfasm_build_global, one batched assembly, D2H of all CSR values."""
+    from lithofem_b200.asm import AsmBatch, AsmGpuGlobal, DeviceVector
+    import copy
+    if a.e2e_steps <= 0:
+        return None
+    ads, h2d = [], 0
+    for c in cases:
+        ad = copy.copy(c.ad)
+        for name in ("dof", "sign", "fo", "attr", "J", "Jinv", "detJ", "v0"):
+            arr = getattr(ad, name)
+            t = torch.empty(arr.shape, dtype=getattr(torch, str(arr.dtype)), pin_memory=True)
+            t.numpy()[...] = arr
+            setattr(ad, name, t.numpy())
+            h2d += arr.nbytes
+        for r in (ad.rule_cc, ad.rule_mass):
+            h2d += r.ip.nbytes + r.w.nbytes + r.vshape.nbytes + r.curl.nbytes
+        h2d += ad.ess.nbytes
+        ads.append(ad)
+    total = sum(c.nnz for c in cases)
+    outs = [torch.empty(2 * c.nnz, dtype=torch.float64, pin_memory=True) for c in cases]
+    times = []
+    for it in range(1 + a.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hs = []
+        for c, ad in zip(cases, ads):
+            g = AsmGpuGlobal(c.prob)
+            assert g.Init(ad, dev) and g.BuildGlobal(ad.ess)
+            hs.append(g)
+        b = AsmBatch(hs)
+        assert b.Assemble(True)
+        for g, o in zip(hs, outs):
+            _, _, V, _, nz = g._csr()
+            o.copy_(torch.as_tensor(DeviceVector(V, (2 * nz,), "<f8"), device="cuda"),
+                    non_blocking=True)
+        torch.cuda.synchronize()
+        b.Release()
+        for g in hs:
+            g.Release()
+        t1 = time.perf_counter()
+        if it >= 1:
+            times.append(t1 - t0)
+    t = float(np.median(times))
+    return {"value": total / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(16 * total), "ms_per_step": 1e3 * t,
+            "what": "per mesh lfasm_init (pinned host arrays) + lfasm_build_global, one "
+                    "lfasm_batch_assemble (graph capture included), D2H of all CSR values",
+            "timer": "host wall clock with device synchronize on both sides"}
+
+
+def cpu_baseline_batch(cases, budget_s: float, threads: int) -> dict:
+    """The reference's CPU reassembler on a bounded sample of every mesh;
+    nnz/s = total nnz / sum of the per-mesh extrapolated times."""
+    t_sum, kinds, elems = 0.0, set(), 0
+    for c in cases:
+        info = cpu_baseline_reference(c, budget_s / len(cases), threads)
+        t_sum += c.nnz / info["value"]
+        kinds.add(info["kind"])
+        elems += int(info["sample"].split(" of ")[0])
+    return {"value": sum(c.nnz for c in cases) / t_sum, "unit": UNIT, "cores": threads,
+            "kind": "reference" if kinds == {"reference"} else "port",
+            "sample": f"{elems} elements over {len(cases)} meshes, reassemble_all per mesh on "
+                      f"its sample's own CSR, extrapolated per mesh"}
+
+
+def run_reference_batch(a, rank, world, dist):
+    from lithofem_b200 import configs
+    from oracle import oracle
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cases = configs.batch_config(scale=a.scale)
+    for c in cases:
+        if oracle.ref_available():
+            rc = oracle.RefContext(c.ad, c.prob)
+            rc.build_csr()
+            c.nnz = rc.nnz
+        else:
+            c.nnz = len(oracle.csr(c.ad)[1])
+    threads = os.cpu_count() or 1
+    vals, info = [], None
+    for it in range(a.warmup + a.steps):
+        info = cpu_baseline_batch(cases, 4.0, threads)
+        if it >= a.warmup:
+            vals.append(info["value"])
+    v = float(np.median(vals))
+    total = sum(c.nnz for c in cases)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": batch_workload_config(cases, a),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -253,6 +253,22 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml);
 
 void lfasm_destroy(lfasm_handle *h);
 
+/* Batched assembly of several meshes on one device (the reference assembles
+ * one mesh per process; no counterpart).  lfasm_batch_create takes n built
+ * handles (lfasm_build_global done) of one device; they must outlive the
+ * batch and keep their structure (no new build, no lfasm_set_bulk_variant)
+ * while it exists.  lfasm_batch_assemble(b, eliminate) has the effect of
+ * lfasm_assemble(h_i, eliminate) on every handle: the first call for an
+ * eliminate flag tunes each handle and captures all of them into one CUDA
+ * graph (one branch per handle, concurrent), later calls launch that graph
+ * once; it returns after the graph has completed on the batch stream
+ * (lfasm_batch_set_stream, default: a stream of the batch). */
+typedef struct lfasm_batch lfasm_batch;
+int lfasm_batch_create(lfasm_handle *const *handles, int n, lfasm_batch **out);
+int lfasm_batch_set_stream(lfasm_batch *b, void *stream);
+int lfasm_batch_assemble(lfasm_batch *b, int eliminate);
+void lfasm_batch_destroy(lfasm_batch *b);
+
 /* Hands the device memory cached by the library's pool on device gpu_id
  * (blocks of destroyed handles and temporaries) back to the driver; live
  * handles keep theirs.  No counterpart in the reference, whose handles

@@ -69,6 +69,10 @@ def lib() -> ct.CDLL:
         "lfasm_get_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
         "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
+        "lfasm_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
+        "lfasm_batch_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+        "lfasm_batch_assemble": (ct.c_int, [ct.c_void_p, ct.c_int]),
+        "lfasm_batch_destroy": (None, [ct.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

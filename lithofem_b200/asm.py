@@ -224,3 +224,41 @@ class AsmGpuGlobal(AsmGpu):
             int(bool(eliminate)), ct.c_void_p(b_ptr)))
         del keep
         return ok
+
+
+class AsmBatch:
+    """Several built ``AsmGpuGlobal`` handles of one device assembled by one
+    CUDA-graph launch (``lfasm_batch_*``).  The handles must outlive the
+    batch; ``Assemble`` has the effect of ``Assemble`` on each of them."""
+
+    def __init__(self, handles: list[AsmGpuGlobal]):
+        self._members = list(handles)
+        self._b = ct.c_void_p()
+        self.last_error = None
+        arr = (ct.c_void_p * max(1, len(handles)))(*[h.handle.value for h in handles])
+        rc = _lib.lib().lfasm_batch_create(arr, len(handles), ct.byref(self._b))
+        if rc != 0:
+            self.last_error = (rc, _lib.lib().lfasm_last_error().decode(errors="replace"))
+            raise RuntimeError(f"lfasm_batch_create: {self.last_error[1]}")
+
+    def SetStream(self, stream_ptr: int) -> bool:
+        return _lib.lib().lfasm_batch_set_stream(self._b, ct.c_void_p(stream_ptr)) == 0
+
+    def Assemble(self, eliminate: bool = True) -> bool:
+        rc = _lib.lib().lfasm_batch_assemble(self._b, int(bool(eliminate)))
+        if rc != 0:
+            self.last_error = (rc, _lib.lib().lfasm_last_error().decode(errors="replace"))
+            print(f"asm_gpu: {self.last_error[1]}", flush=True)
+            return False
+        return True
+
+    def Release(self) -> None:
+        if self._b:
+            _lib.lib().lfasm_batch_destroy(self._b)
+            self._b = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Release()
+        except Exception:  # interpreter shutdown
+            pass

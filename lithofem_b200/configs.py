@@ -1,4 +1,4 @@
-"""Synthetic workloads: the five benchmark stacks and small test cases.
+"""Synthetic workloads: the five benchmark workloads and small test cases.
 
 Geometries follow the benchmark descriptions (EUV, lambda = 13.5 nm,
 absorber n = 0.95 k = 0.031, eps = (n + i k)^2, z-PML of one wavelength,
@@ -16,6 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .mesh import Frustum, Stack, build_mesh, h_for_target_dofs
+from .mesh_poly import PolyHole, build_poly_mesh, random_hole
 from .problem import Problem
 from .space import AsmData, build_asm_data
 
@@ -80,6 +81,62 @@ def make_case(name: str, stack: Stack, p: int, theta: float, ndof_target: float 
     if elem_eps:
         prob.elem_eps = absorber_jitter(ad, prob)
     return Case(name=name, stack=stack, p=p, theta=theta, ad=ad, prob=prob)
+
+
+def make_poly_case(name: str, stack: Stack, p: int, theta: float,
+                   ndof_target: float | None = None, h: float | None = None,
+                   build_csr: bool = False, local_order_seed: int | None = None) -> Case:
+    """A case on the polygon-hole mesh of ``stack`` (its single frustum is a
+    PolyHole); h from the DOF target by one trial build at a coarser h."""
+    hole = stack.frustums[0]
+    prob = Problem.from_stack(stack, p, kpar_of(theta))
+    if h is None:
+        h0 = 1.6 * h_for_target_dofs(stack, p, ndof_target)
+        trial = build_asm_data(build_poly_mesh(stack, hole, h0), p, prob)
+        h = h0 * (trial.height / ndof_target) ** (1.0 / 3.0)
+    mesh = build_poly_mesh(stack, hole, h)
+    ad = build_asm_data(mesh, p, prob, build_csr=build_csr, local_order_seed=local_order_seed)
+    return Case(name=name, stack=stack, p=p, theta=theta, ad=ad, prob=prob)
+
+
+def poly_hole_stack(rng: np.random.Generator, lx: float = 96.0, ly: float = 96.0,
+                    z_max: float = 120.0, t_range=(40.0, 70.0), pml_wl: float = 1.0) -> Stack:
+    """Slab stack with one random polygonal vacuum hole through the absorber:
+    U{3..8} vertices, side wall U(80, 90) deg, absorber thickness U(t_range)."""
+    t = float(rng.uniform(*t_range))
+    nv = int(rng.integers(3, 9))
+    alpha = float(rng.uniform(80.0, 90.0))
+    st = Stack(lx=lx, ly=ly, z_min=0.0, z_max=z_max, wavelength=WAVELENGTH,
+               layers=[(0.0, t, ABSORBER)], pml_thickness_wavelengths=pml_wl)
+    st.frustums = [random_hole(rng, lx, ly, 0.0, t, nv, alpha)]
+    return st
+
+
+def batch_config(scale: float = 1.0, n: int = 16, seed: int = SEED, theta: float = 6.0
+                 ) -> list[Case]:
+    """The batched workload: n seeded polygon-hole meshes, p cycled 1, 2, 3,
+    DOF targets log-uniform in [20k, 400k] (times scale)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        p = 1 + i % 3
+        ndof = float(np.exp(rng.uniform(np.log(20e3), np.log(400e3)))) * scale
+        st = poly_hole_stack(rng)
+        hole = st.frustums[0]
+        name = (f"C5[{i}] polygon hole nv={len(hole.verts)} alpha={hole.alpha:.1f} "
+                f"t={hole.h:.1f} p={p}")
+        out.append(make_poly_case(name, st, p, theta, ndof))
+    return out
+
+
+def small_poly_case(p: int, theta: float, seed: int = 7, h: float | None = None,
+                    local_order_seed: int | None = 7) -> Case:
+    """Seconds-level polygon-hole case (shrunk cell) for the tests."""
+    rng = np.random.default_rng(seed)
+    st = poly_hole_stack(rng, lx=12.0, ly=12.0, z_max=12.0, t_range=(5.0, 7.0), pml_wl=0.4)
+    hh = h if h is not None else {1: 2.0, 2: 3.0, 3: 4.0}[p]
+    return make_poly_case(f"polygon hole p={p} theta={theta}", st, p, theta, h=hh,
+                          build_csr=True, local_order_seed=local_order_seed)
 
 
 def absorber_jitter(ad: AsmData, prob: Problem, seed: int = SEED, frac: float = 0.02

@@ -188,6 +188,7 @@ struct lfasm_handle {
   int ne = 0, nd = 0, p = 0, n = 0, has_kpar = 0;
   int ndp = 0, ndp4 = 0, rs = 0;
   int sm_count = 148;
+  int smem_optin = 48 * 1024;  // max dynamic shared memory per block (opt-in)
   long long nnz = 0;
   // element data
   int *dof = nullptr;
@@ -700,6 +701,7 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   // sector and column pairs fill whole sectors
   LF_CUDA_H(dmalloc(h->Ae, ne * nd * h->rs));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
+  LF_CUDA_H(cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, gpu_id));
   LF_CUDA_H(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   LF_CUDA_H(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
   LF_CUDA_H(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming));
@@ -995,16 +997,22 @@ int lfasm_build_global(lfasm_handle *h, const int *ess_list, int n_ess) {
 }
 
 static int gather(lfasm_handle *h, bool raw, int eliminate) {
-  const int wpb = 8;
+  // one warp per row, each with the row's accumulator in shared memory; the
+  // kernels' dynamic shared memory limit is the device maximum (an upper
+  // bound only), so launches of several handles can share the kernels
+  int wpb = 8;
+  while (wpb > 1 && (size_t)wpb * h->max_row * sizeof(dcplx) > (size_t)h->smem_optin) wpb >>= 1;
   const size_t smem = (size_t)wpb * h->max_row * sizeof(dcplx);
+  if (smem > (size_t)h->smem_optin)
+    return fail(LFASM_ERR_UNSUPPORTED, "CSR row of %d entries exceeds shared memory", h->max_row);
   const unsigned nb = (unsigned)((h->n + wpb - 1) / wpb);
   if (raw) {
-    LF_CUDA(cudaFuncSetAttribute(k_gather<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LF_CUDA(cudaFuncSetAttribute(k_gather<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     k_gather<true><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
                                                       h->Ae, h->nd, h->nd, h->ess, h->sign, h->dof,
                                                       eliminate, h->max_row, h->vals);
   } else {
-    LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     k_gather<false><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
                                                        h->Ae, h->nd, h->rs, h->ess, h->sign, h->dof,
                                                        eliminate, h->max_row, h->vals);
@@ -1134,6 +1142,162 @@ int lfasm_assemble(lfasm_handle *h, int eliminate) {
   if (rc) return rc;
   if (h->profile) LF_CUDA(cudaEventRecord(h->ev[3], h->stream));
   return sync_if(h);
+}
+
+}  // extern "C"
+
+// Batched assembly: several handles (meshes) of one device assembled by one
+// CUDA-graph launch.  The graph holds, per handle, the element kernels and
+// the gather of lfasm_assemble on a branch stream of its own (the PML side
+// stream of the handle joins that branch), all branches forked from and
+// joined into one capture stream, so small meshes run concurrently.
+struct lfasm_batch {
+  int dev = 0;
+  std::vector<lfasm_handle *> hs;
+  cudaStream_t cs = nullptr;         // capture / launch stream
+  cudaStream_t user = nullptr;       // lfasm_batch_set_stream
+  std::vector<cudaStream_t> bs;      // per-handle branch streams
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};  // per eliminate flag
+  long long kernels[2] = {0, 0};                 // kernel nodes per graph
+};
+
+namespace {
+
+void batch_free(lfasm_batch *b) {
+  for (int i = 0; i < 2; ++i)
+    if (b->exec[i]) cudaGraphExecDestroy(b->exec[i]);
+  for (cudaEvent_t e : b->joins)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (cudaStream_t st : b->bs)
+    if (st) cudaStreamDestroy(st);
+  if (b->cs) cudaStreamDestroy(b->cs);
+  delete b;
+}
+
+// capture every handle's fused assembly into one graph
+int batch_capture(lfasm_batch *b, int eliminate) {
+  const int slot = eliminate ? 1 : 0;
+  for (lfasm_handle *h : b->hs)
+    if (!h->tuned) {
+      int rt = lfasm_autotune(h);
+      if (rt) return rt;
+    }
+  LF_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
+  int rc = LFASM_OK;
+  cudaError_t ce = cudaEventRecord(b->fork, b->cs);
+  std::vector<cudaStream_t> keep(b->hs.size());
+  std::vector<int> keep_prof(b->hs.size());
+  for (size_t i = 0; i < b->hs.size() && rc == LFASM_OK && ce == cudaSuccess; ++i) {
+    lfasm_handle *h = b->hs[i];
+    keep[i] = h->stream;
+    keep_prof[i] = h->profile;
+    h->stream = b->bs[i];
+    h->profile = 0;
+    ce = cudaStreamWaitEvent(b->bs[i], b->fork, 0);
+    if (ce == cudaSuccess) {
+      const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
+      rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, eliminate);
+      h->locals_valid = 0;
+      if (rc == LFASM_OK) rc = gather(h, false, eliminate);
+      if (rc == LFASM_OK) ce = cudaEventRecord(b->joins[i], b->bs[i]);
+      if (rc == LFASM_OK && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->cs, b->joins[i], 0);
+    }
+    h->stream = keep[i];
+    h->profile = keep_prof[i];
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->cs, &graph);
+  if (rc != LFASM_OK || ce != cudaSuccess || ee != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != LFASM_OK) return rc;
+    LF_CUDA(ce != cudaSuccess ? ce : ee);
+  }
+  size_t nn = 0;
+  LF_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  LF_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  long long nk = 0;
+  for (cudaGraphNode_t nd_ : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd_, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&b->exec[slot], graph, 0);
+  cudaGraphDestroy(graph);
+  LF_CUDA(ie);
+  b->kernels[slot] = nk;
+  return LFASM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfasm_batch_create(lfasm_handle *const *handles, int n, lfasm_batch **out) {
+  g_err.clear();
+  if (!out) return fail(LFASM_ERR_ARG, "out batch pointer is NULL");
+  *out = nullptr;
+  if (n <= 0 || !handles) return fail(LFASM_ERR_ARG, "empty batch");
+  for (int i = 0; i < n; ++i) {
+    if (!handles[i]) return fail(LFASM_ERR_ARG, "handle %d is NULL", i);
+    if (handles[i]->dev != handles[0]->dev)
+      return fail(LFASM_ERR_ARG, "handle %d is on device %d, handle 0 on %d", i, handles[i]->dev,
+                  handles[0]->dev);
+    if (!handles[i]->built)
+      return fail(LFASM_ERR_STATE, "handle %d: lfasm_build_global has not run", i);
+    for (int j = 0; j < i; ++j)
+      if (handles[j] == handles[i]) return fail(LFASM_ERR_ARG, "handle %d repeats handle %d", i, j);
+  }
+  LF_CUDA(cudaSetDevice(handles[0]->dev));
+  lfasm_batch *b = new lfasm_batch();
+  b->dev = handles[0]->dev;
+  b->hs.assign(handles, handles + n);
+  b->bs.assign(n, nullptr);
+  b->joins.assign(n, nullptr);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&b->bs[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    batch_free(b);
+    LF_CUDA(e);
+  }
+  *out = b;
+  return LFASM_OK;
+}
+
+int lfasm_batch_set_stream(lfasm_batch *b, void *stream) {
+  if (!b) return fail(LFASM_ERR_ARG, "NULL batch");
+  b->user = (cudaStream_t)stream;
+  return LFASM_OK;
+}
+
+int lfasm_batch_assemble(lfasm_batch *b, int eliminate) {
+  if (!b) return fail(LFASM_ERR_ARG, "NULL batch");
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(b->dev));
+  const int slot = eliminate ? 1 : 0;
+  if (!b->exec[slot]) {
+    int rc = batch_capture(b, eliminate);
+    if (rc) return rc;
+  }
+  cudaStream_t st = b->user ? b->user : b->cs;
+  LF_CUDA(cudaGraphLaunch(b->exec[slot], st));
+  g_launches.fetch_add(b->kernels[slot], std::memory_order_relaxed);
+  LF_CUDA(cudaStreamSynchronize(st));
+  return LFASM_OK;
+}
+
+void lfasm_batch_destroy(lfasm_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->cs) cudaStreamSynchronize(b->cs);
+  if (b->user) cudaStreamSynchronize(b->user);
+  batch_free(b);
 }
 
 int lfasm_set_profile(lfasm_handle *h, int on) {
