@@ -516,6 +516,7 @@ def run_batch(a, rank, world, local, dist, torch):
     # per-mesh stage profile (serial, untimed) and the serial per-handle time
     stages = np.zeros(3)
     serial_ms = 0.0
+    per_mesh = []
     for g in hs:
         assert g.Assemble(True)          # tunes the handle
         assert g.SetProfile(True)
@@ -523,6 +524,7 @@ def run_batch(a, rank, world, local, dist, torch):
         st = np.array(g.StageTimes())
         stages += st
         serial_ms += float(st.sum())
+        per_mesh.append([round(float(x), 4) for x in st])
         assert g.SetProfile(False)
     b = AsmBatch(hs)
     assert b.SetStream(stream.cuda_stream)
@@ -593,7 +595,8 @@ def run_batch(a, rank, world, local, dist, torch):
             "config": batch_workload_config(cases, a), "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
             "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
-            "serial_per_handle_ms": serial_ms}
+            "serial_per_handle_ms": serial_ms,
+            "per_mesh_stage_ms": per_mesh}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

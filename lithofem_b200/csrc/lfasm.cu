@@ -227,6 +227,9 @@ struct lfasm_handle {
   int *ea_ptr = nullptr, *ea = nullptr;
   uint16_t *off = nullptr;
   int max_row = 0;
+  int row_cap = 0;            // gather: rows up to row_cap entries in shared memory
+  int *long_rows = nullptr;   // the longer rows
+  int n_long = 0;
   double *partials = nullptr, *red = nullptr;
   int n_part_blocks = 0;
   // optional per-stage events of lfasm_assemble: prep+bulk, pml, gather
@@ -960,6 +963,22 @@ static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long n
   if (herr) return fail(LFASM_ERR_UNSUPPORTED, "row map overflow");
   if (mrow > 65535) return fail(LFASM_ERR_UNSUPPORTED, "row with %d entries exceeds 65535", mrow);
   h->max_row = std::max(mrow, 1);
+  // gather: rows up to GATHER_ROW_CAP entries accumulate in shared memory
+  constexpr int GATHER_ROW_CAP = 256;
+  h->row_cap = std::min(h->max_row, GATHER_ROW_CAP);
+  h->n_long = 0;
+  if (h->max_row > h->row_cap) {
+    int *cnt_d = nullptr;
+    LF_CUDA(dmalloc(cnt_d, 1));
+    LF_CUDA(dmalloc(h->long_rows, (size_t)n));
+    LF_CUDA(cudaMemsetAsync(cnt_d, 0, sizeof(int), h->stream));
+    k_long_rows<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(n, h->I, h->row_cap,
+                                                                   h->long_rows, cnt_d);
+    LF_LAUNCHED();
+    LF_CUDA(cudaMemcpyAsync(&h->n_long, cnt_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    LF_CUDA(cudaStreamSynchronize(h->stream));
+    dfree(cnt_d);
+  }
   return LFASM_OK;
 }
 
@@ -997,27 +1016,35 @@ int lfasm_build_global(lfasm_handle *h, const int *ess_list, int n_ess) {
 }
 
 static int gather(lfasm_handle *h, bool raw, int eliminate) {
-  // one warp per row, each with the row's accumulator in shared memory; the
-  // kernels' dynamic shared memory limit is the device maximum (an upper
-  // bound only), so launches of several handles can share the kernels
-  int wpb = 8;
-  while (wpb > 1 && (size_t)wpb * h->max_row * sizeof(dcplx) > (size_t)h->smem_optin) wpb >>= 1;
-  const size_t smem = (size_t)wpb * h->max_row * sizeof(dcplx);
-  if (smem > (size_t)h->smem_optin)
-    return fail(LFASM_ERR_UNSUPPORTED, "CSR row of %d entries exceeds shared memory", h->max_row);
+  // one warp per row, each with the row's accumulator in shared memory
+  // (h->row_cap entries); the few longer rows (h->long_rows) go to a second,
+  // small launch that accumulates in place in global memory, so that they do
+  // not cut the occupancy of the whole gather.  The kernels' dynamic shared
+  // memory limit is the device maximum (an upper bound only), so launches of
+  // several handles can share the kernels.
+  const int cap = h->row_cap;
+  const int wpb = 8;
+  const size_t smem = (size_t)wpb * cap * sizeof(dcplx);
   const unsigned nb = (unsigned)((h->n + wpb - 1) / wpb);
+  const unsigned nl = (unsigned)((h->n_long + wpb - 1) / wpb);
+  const int rs = raw ? h->nd : h->rs;
+#define LF_GATHER(R, L, grid, rows, sm)                                                       \
+  k_gather<R, L><<<grid, wpb * 32, sm, h->stream>>>(rows, h->long_rows, h->ea_ptr, h->ea,      \
+                                                    h->off, h->I, h->Jc, h->Ae, h->nd, rs,     \
+                                                    h->ess, h->sign, h->dof, eliminate, cap,   \
+                                                    h->vals)
   if (raw) {
-    LF_CUDA(cudaFuncSetAttribute(k_gather<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
-    k_gather<true><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
-                                                      h->Ae, h->nd, h->nd, h->ess, h->sign, h->dof,
-                                                      eliminate, h->max_row, h->vals);
+    LF_CUDA(cudaFuncSetAttribute(k_gather<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    LF_GATHER(true, false, nb, h->n, smem);
+    LF_LAUNCHED();
+    if (h->n_long) { LF_GATHER(true, true, nl, h->n_long, 0); LF_LAUNCHED(); }
   } else {
-    LF_CUDA(cudaFuncSetAttribute(k_gather<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
-    k_gather<false><<<nb, wpb * 32, smem, h->stream>>>(h->n, h->ea_ptr, h->ea, h->off, h->I, h->Jc,
-                                                       h->Ae, h->nd, h->rs, h->ess, h->sign, h->dof,
-                                                       eliminate, h->max_row, h->vals);
+    LF_CUDA(cudaFuncSetAttribute(k_gather<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
+    LF_GATHER(false, false, nb, h->n, smem);
+    LF_LAUNCHED();
+    if (h->n_long) { LF_GATHER(false, true, nl, h->n_long, 0); LF_LAUNCHED(); }
   }
-  LF_LAUNCHED();
+#undef LF_GATHER
   return LFASM_OK;
 }
 
@@ -1603,7 +1630,7 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
   dfree(h->S); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
-  dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->off); dfree(h->partials);
+  dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->long_rows); dfree(h->off); dfree(h->partials);
   dfree(h->red);
   for (int i = 0; i < 4; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);

@@ -878,24 +878,44 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 // through the precomputed entry -> slot-offset map (no atomics).
 // RAW: element buffer without signs/elimination (ComputeLocal output).
 // ---------------------------------------------------------------------------
+// The row's element contributions summed into acc[0..nr) (shared memory, or
+// the row's own CSR values for rows longer than the shared accumulator),
+// the unit diagonal of an essential row set.  Inlined twice so that the
+// shared-memory path keeps shared-memory instructions.
 template <bool RAW>
-__global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__restrict__ ea,
-                         const uint16_t *__restrict__ off, const int *__restrict__ I,
-                         const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd, int rs,
-                         const unsigned char *__restrict__ ess,
-                         const double *__restrict__ sign, const int *__restrict__ dof,
-                         int eliminate, int maxrow, dcplx *__restrict__ vals) {
-  extern __shared__ dcplx sacc[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int r = blockIdx.x * (blockDim.x >> 5) + wib;
-  if (r >= n) return;
-  dcplx *acc = sacc + (size_t)wib * maxrow;
-  const int rb = I[r], nr = I[r + 1] - rb;
+__device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, int lane,
+                                           const int *__restrict__ ea_ptr,
+                                           const int *__restrict__ ea,
+                                           const uint16_t *__restrict__ off,
+                                           const int *__restrict__ Jc,
+                                           const dcplx *__restrict__ Ae, int nd, int rs,
+                                           const unsigned char *__restrict__ ess,
+                                           const double *__restrict__ sign,
+                                           const int *__restrict__ dof, int eliminate) {
   for (int j = lane; j < nr; j += 32) acc[j] = mk(0.0, 0.0);
   __syncwarp();
   const bool row_ess = eliminate && ess[r];
   const int p1 = ea_ptr[r + 1];
-  {
+  if (!RAW && nd <= 16) {
+    // short element rows (p = 1): 32 / nd row-list entries per pass, one
+    // lane per (entry, column); their loads issue together, the additions
+    // go entry by entry (two entries may share a slot)
+    const int epi = 32 / nd;
+    const int sub = lane / nd, b = lane - sub * nd;
+    for (int q0 = ea_ptr[r]; q0 < p1; q0 += epi) {
+      const int pp = q0 + sub;
+      dcplx v = mk(0.0, 0.0);
+      int j = -1;
+      if (sub < epi && pp < p1) {
+        v = Ae[(size_t)ea[pp] * rs + b];
+        j = off[(size_t)pp * nd + b];
+      }
+      for (int t = 0; t < epi; ++t) {
+        if (sub == t && j >= 0) { acc[j].re += v.re; acc[j].im += v.im; }
+        __syncwarp();
+      }
+    }
+  } else {
     for (int pp = ea_ptr[r]; pp < p1; ++pp) {
       const int id = ea[pp];
       const dcplx *src = Ae + (size_t)id * rs;
@@ -926,7 +946,39 @@ __global__ void k_gather(int n, const int *__restrict__ ea_ptr, const int *__res
     acc[lo] = mk(1.0, 0.0);
   }
   __syncwarp();
-  for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
+}
+
+// LONG = false: one warp per row r < n, accumulator in shared memory; rows
+// longer than maxrow are skipped.  LONG = true: one warp per entry of
+// long_rows (the rows longer than maxrow), accumulating in place in the
+// row's CSR values, still owned by this warp alone.
+template <bool RAW, bool LONG>
+__global__ void k_gather(int n, const int *__restrict__ long_rows, const int *__restrict__ ea_ptr,
+                         const int *__restrict__ ea,
+                         const uint16_t *__restrict__ off, const int *__restrict__ I,
+                         const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd, int rs,
+                         const unsigned char *__restrict__ ess,
+                         const double *__restrict__ sign, const int *__restrict__ dof,
+                         int eliminate, int maxrow, dcplx *__restrict__ vals) {
+  extern __shared__ dcplx sacc[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (w >= n) return;
+  const int r = LONG ? long_rows[w] : w;
+  const int rb = I[r], nr = I[r + 1] - rb;
+  if (!LONG && nr > maxrow) return;
+  dcplx *acc = LONG ? vals + rb : sacc + (size_t)wib * maxrow;
+  gather_row<RAW>(acc, r, rb, nr, lane, ea_ptr, ea, off, Jc, Ae, nd, rs, ess, sign, dof,
+                  eliminate);
+  if (!LONG)
+    for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
+}
+
+// rows longer than cap, in any order
+__global__ void k_long_rows(int n, const int *__restrict__ I, int cap, int *__restrict__ out,
+                            int *__restrict__ count) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n && I[r + 1] - I[r] > cap) out[atomicAdd(count, 1)] = r;
 }
 
 // ---------------------------------------------------------------------------

@@ -233,7 +233,8 @@ def build_poly_mesh(stack: Stack, hole: PolyHole, h: float) -> TetMesh:
     s0 = cum[pe] + pu * elen[pe]  # arc position of ring-0 nodes
     for k in range(1, K):
         frac = 1.0 - k / K
-        nk = max(3, int(round(nr * frac)))
+        # point spacing ~h along every ring: the centre fan stays small
+        nk = max(3, min(nr, int(round(perim * frac / h))))
         start = s0[0]
         ids = []
         for m in range(nk):
