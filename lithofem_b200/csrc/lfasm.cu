@@ -738,7 +738,7 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
 template <int NDP8>
 static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int mask_mass, int te,
                       int eliminate, int rs, cudaStream_t st) {
-  const size_t smem = PmlShape<NDP8>::SMEM;
+  const size_t smem = PmlShape<NDP8>::smem(PmlShape<NDP8>::QC, h->rcc.nq + h->rm.nq);
   const int threads = NDP8 * 4;
   auto go = [&](auto kern) -> int {
     LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

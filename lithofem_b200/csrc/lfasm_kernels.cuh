@@ -618,7 +618,7 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
 // A[m][r] = X[r][m], B[r][n] = Yre/Yim[r][n]; M = N = NDP8 (nd rounded up
 // to 8).  One warp per 8-column tile (real and imaginary planes), all
 // M tiles, so the epilogue holds both parts of each entry.  Rows are staged
-// in chunks of PML_QC points; blocks are persistent over the PML elements.
+// in chunks of 8 points (p = 3) or 4; blocks are persistent over the PML elements.
 //
 // The stretch coefficients of every point of both rules (one pow() each)
 // are formed once per element by all threads in parallel, into a table in
@@ -642,12 +642,16 @@ struct PmlShape {
   // (g, t4) reads row r0 + t4, column 8 m + g) then fall on 16 distinct
   // 8-byte bank pairs in each half-warp
   static constexpr int LD = NDP8 + ((4 - NDP8 % 16) + 16) % 16;
-  static constexpr int RMAX = PML_QC * 6;                // rows per chunk (multiple of 4)
-  static constexpr size_t SMEM =
-      (size_t)3 * RMAX * LD * sizeof(double) + PML_MAXQ * sizeof(QCoef);
+  // points per chunk: 8 at p = 3, 4 below (smaller blocks, more per SM)
+  static constexpr int QC = NDP8 >= 48 ? PML_QC : 4;
+  // shared memory for chunks of qc points (rmax = 6 qc staged rows) and a
+  // coefficient table of nq_all points
+  static size_t smem(int qc, int nq_all) {
+    return (size_t)3 * (6 * qc) * LD * sizeof(double) + (size_t)nq_all * sizeof(QCoef);
+  }
   // blocks per SM the register budget is cut for (shared memory allows it)
   // p = 3 stays at 2 blocks (a 3-block register cap spills and runs slower)
-  static constexpr int MINB = NDP8 >= 48 ? 2 : NDP8 >= 24 ? 4 : 8;
+  static constexpr int MINB = NDP8 >= 48 ? 2 : NDP8 >= 24 ? 5 : 16;
 };
 
 // Coefficients of one quadrature point (rule 0: curl-curl, rule 1: mass and
@@ -703,7 +707,7 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
           const unsigned long long *__restrict__ signmask,
           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
   using Sh = PmlShape<NDP8>;
-  constexpr int LD = Sh::LD, MT = Sh::MT, RMAX = Sh::RMAX;
+  constexpr int LD = Sh::LD, MT = Sh::MT, QC = Sh::QC, RMAX = 6 * QC;
   extern __shared__ double smem[];
   double *Xs = smem;
   double *Yr = Xs + RMAX * LD;
@@ -746,8 +750,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
       const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
       const bool need_v = rule == 1;
       const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
-      for (int q0 = 0; q0 < R.nq; q0 += PML_QC) {
-        const int nqc = min(PML_QC, R.nq - q0);
+      for (int q0 = 0; q0 < R.nq; q0 += QC) {
+        const int nqc = min(QC, R.nq - q0);
         const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
         // zero the padding rows up to a multiple of 4
         for (int i = tid; i < (nrows4 - nrows) * LD; i += blockDim.x) {
