@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pml-variant", type=int, default=-1,
+                    help="force the p = 3 PML kernel (0 k_pml_mma, 1 k_pml_ws); default: autotune")
     ap.add_argument("--bulk-variant", type=int, default=-1,
                     help="force the bulk-element kernel (0 SIMT, 1 DMMA); default: autotune")
     return ap.parse_args()
@@ -307,7 +309,10 @@ def run_ours(a, rank, world, local, dist, torch):
     assert g.Autotune()
     if a.bulk_variant >= 0:
         assert g.SetBulkVariant(a.bulk_variant)
+    if a.pml_variant >= 0:
+        assert g.SetPmlVariant(a.pml_variant)
     tuning = g.Tuning()
+    pml_tuning = g.PmlTuning()
     # warm-up
     for _ in range(a.warmup):
         assert g.Assemble(True)
@@ -423,7 +428,9 @@ def run_ours(a, rank, world, local, dist, torch):
             "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
             "tuning": {"bulk_variant": ["k_bulk (SIMT)", "k_bulk_mma<4 tiles/warp> (DMMA)",
                                         "k_bulk_mma<2 tiles/warp> (DMMA)"][tuning[0]],
-                       "bulk_ms": tuning[1]}}
+                       "bulk_ms": tuning[1],
+                       "pml_variant": ["k_pml_mma", "k_pml_ws (warp-specialised)"][pml_tuning[0]],
+                       "pml_ms": pml_tuning[1]}}
     print(json.dumps(line), flush=True)
     g.Release()
     if dist is not None:

@@ -239,6 +239,13 @@ int lfasm_autotune(lfasm_handle *h);
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant);
 int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3);
 
+/* The PML-element kernel at p = 3: 0 k_pml_mma, 1 k_pml_ws (warp-specialised
+ * producer/consumer pipeline).  The autotuner times both on the mesh (the
+ * cached decision carries it); lfasm_set_pml_variant fixes it (1 only at
+ * p = 3).  lfasm_get_pml_tuning reports the choice and both timings (ms). */
+int lfasm_set_pml_variant(lfasm_handle *h, int variant);
+int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms2);
+
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
  * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the

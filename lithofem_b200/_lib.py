@@ -67,6 +67,8 @@ def lib() -> ct.CDLL:
         "lfasm_autotune": (ct.c_int, [H]),
         "lfasm_set_bulk_variant": (ct.c_int, [H, ct.c_int]),
         "lfasm_get_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
+        "lfasm_set_pml_variant": (ct.c_int, [H, ct.c_int]),
+        "lfasm_get_pml_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
         "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
         "lfasm_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),

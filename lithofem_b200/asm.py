@@ -108,6 +108,15 @@ class AsmGpu:
         _lib.check(_lib.lib().lfasm_get_tuning(self._h, ct.byref(v), ms))
         return v.value, [float(x) for x in ms]
 
+    def SetPmlVariant(self, variant: int) -> bool:
+        return self._ok(_lib.lib().lfasm_set_pml_variant(self._h, int(variant)))
+
+    def PmlTuning(self) -> tuple[int, list[float]]:
+        v = ct.c_int()
+        ms = (ct.c_float * 2)()
+        _lib.check(_lib.lib().lfasm_get_pml_tuning(self._h, ct.byref(v), ms))
+        return v.value, [float(x) for x in ms]
+
     def PathCounts(self) -> tuple[int, int]:
         a, b = ct.c_int(), ct.c_int()
         _lib.check(_lib.lib().lfasm_path_counts(self._h, ct.byref(a), ct.byref(b)))

@@ -211,6 +211,11 @@ struct lfasm_handle {
   int tuned = 0;             // autotune done
   int forced = 0;            // variant fixed by lfasm_set_bulk_variant
   float tune_ms[3] = {0.f, 0.f, 0.f};
+  // PML kernel at p = 3: 0 k_pml_mma, 1 k_pml_ws (warp-specialised)
+  int pml_variant = 0;
+  int pml_forced = 0;
+  float pml_ms[2] = {0.f, 0.f};
+  int *err = nullptr;  // device error word of the bounded-wait kernels
   dcplx *Ae = nullptr;
   // RHS data
   int *slab_of = nullptr;
@@ -246,7 +251,17 @@ namespace {
 
 int sync_if(lfasm_handle *h) {
   LF_CUDA(cudaGetLastError());
-  if (!h->async_mode) LF_CUDA(cudaStreamSynchronize(h->stream));
+  if (!h->async_mode) {
+    LF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->pml_variant == 1 && h->err) {
+      int e = 0;
+      LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (e) {
+        LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+        return fail(LFASM_ERR_CUDA, "PML pipeline: a bounded wait ran out (results undefined)");
+      }
+    }
+  }
   return LFASM_OK;
 }
 
@@ -703,6 +718,8 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   // stride ndp (even) for the fused path so every row starts on a 32-byte
   // sector and column pairs fill whole sectors
   LF_CUDA_H(dmalloc(h->Ae, ne * nd * h->rs));
+  LF_CUDA_H(dmalloc(h->err, 1));
+  LF_CUDA_H(cudaMemset(h->err, 0, sizeof(int)));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, gpu_id));
   LF_CUDA_H(cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, gpu_id));
   LF_CUDA_H(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -752,6 +769,21 @@ static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int ma
     LF_LAUNCHED();
     return LFASM_OK;
   };
+  if (NDP8 == 48 && h->pml_variant == 1) {
+    const size_t wsm = PmlWsShape::smem(h->rcc.nq + h->rm.nq);
+    auto ws = [&](auto kern) -> int {
+      LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+      const int grid = std::max(1, std::min(h->n_pml, h->sm_count));
+      kern<<<grid, WS_THREADS, wsm, st>>>(
+          h->n_pml, h->pml_list, h->nd, rs, h->p, h->rcc.view(), h->rm.view(), h->J, h->Jinv,
+          h->detJ, h->v0, h->attr, h->eps_tab, h->elem_eps, h->pml, mask_cc, mask_mass, te,
+          eliminate, h->fopack, h->signmask, h->essmask, h->Ae, h->err);
+      LF_LAUNCHED();
+      return LFASM_OK;
+    };
+    if (cross) return mode ? ws(k_pml_ws<true, 1>) : ws(k_pml_ws<true, 0>);
+    return mode ? ws(k_pml_ws<false, 1>) : ws(k_pml_ws<false, 0>);
+  }
   if (cross) return mode ? go(k_pml_mma<NDP8, true, 1>) : go(k_pml_mma<NDP8, true, 0>);
   return mode ? go(k_pml_mma<NDP8, false, 1>) : go(k_pml_mma<NDP8, false, 0>);
 }
@@ -1067,6 +1099,8 @@ namespace {
 struct TuneEntry {
   int variant;
   float ms[3];
+  int pml_variant;
+  float pml_ms[2];
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 4>, TuneEntry> g_tune;
@@ -1106,13 +1140,38 @@ int lfasm_autotune(lfasm_handle *h) {
     }
   }
   h->n_pml = keep_n_pml;
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  if (rc) return rc;
   int best = 0;
   for (int v = 1; v < 3; ++v)
     if (h->tune_ms[v] < h->tune_ms[best]) best = v;
   h->bulk_variant = best;
+  if (!rc && h->p == 3 && h->n_pml > 0 && !h->pml_forced) {
+    // PML kernels at p = 3, the PML path alone
+    const int keep_n_bulk = h->n_bulk;
+    h->n_bulk = 0;
+    for (int v = 0; v < 2 && !rc; ++v) {
+      h->pml_variant = v;
+      for (int rep = 0; rep < 2 && !rc; ++rep) {
+        LF_CUDA(cudaEventRecord(a, h->stream));
+        rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, 1);
+        LF_CUDA(cudaEventRecord(b, h->stream));
+      }
+      if (!rc) {
+        LF_CUDA(cudaEventSynchronize(b));
+        LF_CUDA(cudaEventElapsedTime(&h->pml_ms[v], a, b));
+      }
+    }
+    h->n_bulk = keep_n_bulk;
+    if (!rc) {
+      int e = 0;
+      LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+      // a variant whose waits ran out is never chosen
+      h->pml_variant = (e == 0 && h->pml_ms[1] < h->pml_ms[0]) ? 1 : 0;
+      if (e) LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
   h->tuned = 1;
   h->locals_valid = 0;
   {
@@ -1120,6 +1179,9 @@ int lfasm_autotune(lfasm_handle *h) {
     TuneEntry &t = g_tune[tune_key(h)];
     t.variant = best;
     for (int v = 0; v < 3; ++v) t.ms[v] = h->tune_ms[v];
+    t.pml_variant = h->pml_variant;
+    t.pml_ms[0] = h->pml_ms[0];
+    t.pml_ms[1] = h->pml_ms[1];
   }
   return sync_if(h);
 }
@@ -1130,6 +1192,23 @@ int lfasm_set_bulk_variant(lfasm_handle *h, int variant) {
   h->bulk_variant = variant;
   h->forced = 1;
   h->tuned = 1;
+  return LFASM_OK;
+}
+
+int lfasm_set_pml_variant(lfasm_handle *h, int variant) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (variant < 0 || variant > 1) return fail(LFASM_ERR_ARG, "PML variant must be 0 or 1");
+  if (variant == 1 && h->p != 3)
+    return fail(LFASM_ERR_UNSUPPORTED, "the warp-specialised PML kernel is for p = 3");
+  h->pml_variant = variant;
+  h->pml_forced = 1;
+  return LFASM_OK;
+}
+
+int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms2) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (pml_variant) *pml_variant = h->pml_variant;
+  if (ms2) for (int i = 0; i < 2; ++i) ms2[i] = h->pml_ms[i];
   return LFASM_OK;
 }
 
@@ -1153,6 +1232,9 @@ int lfasm_assemble(lfasm_handle *h, int eliminate) {
         hit = true;
         h->bulk_variant = it->second.variant;
         for (int v = 0; v < 3; ++v) h->tune_ms[v] = it->second.ms[v];
+        if (!h->pml_forced) h->pml_variant = it->second.pml_variant;
+        h->pml_ms[0] = it->second.pml_ms[0];
+        h->pml_ms[1] = it->second.pml_ms[1];
         h->tuned = 1;
       }
     }
@@ -1316,6 +1398,16 @@ int lfasm_batch_assemble(lfasm_batch *b, int eliminate) {
   LF_CUDA(cudaGraphLaunch(b->exec[slot], st));
   g_launches.fetch_add(b->kernels[slot], std::memory_order_relaxed);
   LF_CUDA(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < b->hs.size(); ++i) {
+    lfasm_handle *h = b->hs[i];
+    if (h->pml_variant != 1) continue;
+    int e = 0;
+    LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+      return fail(LFASM_ERR_CUDA, "handle %zu: PML pipeline: a bounded wait ran out", i);
+    }
+  }
   return LFASM_OK;
 }
 
@@ -1628,7 +1720,7 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
   for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
-  dfree(h->S); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
+  dfree(h->S); dfree(h->err); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
   dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->long_rows); dfree(h->off); dfree(h->partials);
   dfree(h->red);

@@ -696,6 +696,86 @@ __device__ __forceinline__ QCoef pml_qcoef(const PmlParams &pml, int rule, int m
   return c;
 }
 
+// One staged pair of PML rows: element-local columns k = 2 pr, 2 pr + 1 of
+// quadrature point q (chunk row block qi): physical shapes/curls, the dual
+// face transform, and X (real), Y = W X (two planes) at row stride LD.
+template <int LD>
+__device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule &R, int nd, int p,
+                                               int te, bool need_v, bool need_c, int rule, int rq,
+                                               const double *sJ, const double *sJi, double sidet,
+                                               unsigned sfo, const QCoef &C, double *Xs,
+                                               double *Yr, double *Yi) {
+  double v[2][3], c[2][3];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = 2 * pr + h;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
+    if (k < nd) {
+      const double *rv = R.v + ((size_t)q * nd + k) * 3;
+      const double *rc = R.c + ((size_t)q * nd + k) * 3;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (need_v)
+          v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
+        if (need_c)
+          c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) * sidet;
+      }
+    }
+  }
+  if (te && p >= 2) {
+    const int f = face_of(2 * pr, p);
+    if (f >= 0) {
+      const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
+        v[0][d] = v0_ * T[0] + v1_ * T[1];
+        v[1][d] = v0_ * T[2] + v1_ * T[3];
+        c[0][d] = c0_ * T[0] + c1_ * T[1];
+        c[1][d] = c0_ * T[2] + c1_ * T[3];
+      }
+    }
+  }
+  
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = 2 * pr + h;
+    const int rb = qi * rq;
+    if (rule == 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
+      const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
+                  y2 = cscale(c[h][2], C.a22);
+      Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+      Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+      Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+    } else {
+      const double *vv = v[h], *cc = c[h];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
+      dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+      dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+      dcplx y2 = cscale(vv[2], C.a22);
+      if (need_c) {
+        y0 = cadd(y0, cscale(cc[2], C.b02));
+        y1 = cadd(y1, cscale(cc[2], C.b12));
+        y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
+        const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
+                    z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+        Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
+        Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
+        Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
+      }
+      Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+      Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+      Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+    }
+  }
+}
+
 template <int NDP8, bool CROSS, int MODE>
 __global__ void __launch_bounds__(NDP8 * 4, PmlShape<NDP8>::MINB)
 k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
@@ -760,76 +840,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
         }
         for (int it = tid; it < nqc * npair; it += blockDim.x) {
           const int qi = it / npair, pr = it - qi * npair;
-          const int q = q0 + qi;
-          double v[2][3], c[2][3];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int k = 2 * pr + h;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
-            if (k < nd) {
-              const double *rv = R.v + ((size_t)q * nd + k) * 3;
-              const double *rc = R.c + ((size_t)q * nd + k) * 3;
-#pragma unroll
-              for (int d = 0; d < 3; ++d) {
-                if (need_v)
-                  v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
-                if (need_c)
-                  c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) * sidet;
-              }
-            }
-          }
-          if (te && p >= 2) {
-            const int f = face_of(2 * pr, p);
-            if (f >= 0) {
-              const double *T = c_tinv + 4 * ((sfo >> (8 * f)) & 0xffu);
-#pragma unroll
-              for (int d = 0; d < 3; ++d) {
-                const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
-                v[0][d] = v0_ * T[0] + v1_ * T[1];
-                v[1][d] = v0_ * T[2] + v1_ * T[3];
-                c[0][d] = c0_ * T[0] + c1_ * T[1];
-                c[1][d] = c0_ * T[2] + c1_ * T[3];
-              }
-            }
-          }
-          const QCoef &C = qc[q];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int k = 2 * pr + h;
-            const int rb = qi * rq;
-            if (rule == 0) {
-#pragma unroll
-              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
-              const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
-                          y2 = cscale(c[h][2], C.a22);
-              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
-            } else {
-              const double *vv = v[h], *cc = c[h];
-#pragma unroll
-              for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
-              dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
-              dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
-              dcplx y2 = cscale(vv[2], C.a22);
-              if (need_c) {
-                y0 = cadd(y0, cscale(cc[2], C.b02));
-                y1 = cadd(y1, cscale(cc[2], C.b12));
-                y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
-#pragma unroll
-                for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
-                const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
-                            z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
-                Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
-                Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
-                Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
-              }
-              Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-              Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-              Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
-            }
-          }
+          pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, sJ, sJi,
+                             sidet, sfo, qc[q0 + qi], Xs, Yr, Yi);
         }
         __syncthreads();
         // tensor-core contraction of the staged rows
@@ -854,6 +866,208 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
       const int row = m * 8 + g;
+      if (row >= nd) continue;
+      dcplx v2[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int l = col + i;
+        double re = cr[m][i], im = ci[m][i];
+        if (MODE == 1) {
+          const double sg = ((((sm >> row) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
+          re *= sg; im *= sg;
+          if (((em >> row) | (em >> l)) & 1ull) { re = 0.0; im = 0.0; }
+        }
+        v2[i] = mk(re, im);
+      }
+      if (col + 1 < nd) {
+        dst[(size_t)row * rs + col] = v2[0];
+        dst[(size_t)row * rs + col + 1] = v2[1];
+      } else if (col < nd) {
+        dst[(size_t)row * rs + col] = v2[0];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PML elements at p = 3, warp-specialised (alternative to k_pml_mma<48>,
+// chosen by the autotuner).  Four producer warps stage the rows of chunk
+// c + 1 into one half of a double buffer while twelve consumer warps run the
+// DMMA contraction of chunk c from the other half; each consumer warp owns
+// three row tiles of one 8-column tile (real and imaginary planes).  The
+// halves are handed over through mbarriers (full: every producer thread
+// arrives after its stores; empty: every consumer thread arrives after its
+// loads).  Every wait is bounded: a wait that runs out sets *err, and that
+// thread then skips its remaining waits but keeps to the same loop, so the
+// kernel always finishes (with the error reported, results undefined).
+// ---------------------------------------------------------------------------
+constexpr int WS_CONS = 12, WS_PROD = 4;
+constexpr int WS_THREADS = (WS_CONS + WS_PROD) * 32;
+constexpr long long WS_WAIT_LIMIT = 1ll << 20;  // try_wait rounds before giving up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the completion of the phase with the given parity;
+// false (and *err set) if it did not complete
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int *err) {
+  for (long long it = 0; it < WS_WAIT_LIMIT; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
+struct PmlWsShape {
+  static constexpr int NDP8 = 48, LD = 52, MT = 6, QC = 8, RMAX = 6 * QC;
+  static constexpr size_t BUF = (size_t)3 * RMAX * LD;  // doubles per buffer half
+  static size_t smem(int nq_all) {
+    return 2 * BUF * sizeof(double) + (size_t)nq_all * sizeof(QCoef);
+  }
+};
+
+template <bool CROSS, int MODE>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
+         const double *__restrict__ J9, const double *__restrict__ Ji9,
+         const double *__restrict__ detJ, const double *__restrict__ v0,
+         const int *__restrict__ attr, const dcplx *__restrict__ eps_tab,
+         const dcplx *__restrict__ elem_eps, PmlParams pml, int mask_cc, int mask_mass, int te,
+         int eliminate, const unsigned *__restrict__ fopack,
+         const unsigned long long *__restrict__ signmask,
+         const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae,
+         int *__restrict__ err) {
+  using Sh = PmlWsShape;
+  constexpr int LD = Sh::LD, QC = Sh::QC, RMAX = Sh::RMAX, NDP8 = Sh::NDP8;
+  extern __shared__ double smem[];
+  QCoef *qtab = reinterpret_cast<QCoef *>(smem + 2 * Sh::BUF);
+  __shared__ unsigned long long full[2], empty[2];
+  __shared__ double sJ[9], sJi[9], sidet;
+  __shared__ unsigned sfo;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    mbar_init(&full[0], WS_PROD * 32);
+    mbar_init(&full[1], WS_PROD * 32);
+    mbar_init(&empty[0], WS_CONS * 32);
+    mbar_init(&empty[1], WS_CONS * 32);
+  }
+  __syncthreads();
+  const int nq_all = rcc.nq + rm.nq;
+  bool live = true;  // false after a wait ran out: no more waiting
+
+  if (warp >= WS_CONS) {
+    // ------------------------------------------------------------ producers
+    const int ptid = tid - WS_CONS * 32;
+    constexpr int npair = NDP8 / 2;
+    unsigned c = 0;
+    for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
+      const int e = list[ie];
+      if (ptid < 9) { sJ[ptid] = J9[(size_t)e * 9 + ptid]; sJi[ptid] = Ji9[(size_t)e * 9 + ptid]; }
+      if (ptid == 0) { sidet = 1.0 / detJ[e]; sfo = fopack[e]; }
+      for (int j = ptid; j < nq_all; j += WS_PROD * 32) {
+        const int rule = j < rcc.nq ? 0 : 1;
+        const int q = rule == 0 ? j : j - rcc.nq;
+        const Rule &R = rule == 0 ? rcc : rm;
+        const double *Jz = J9 + (size_t)e * 9 + 6;
+        const double z = v0[(size_t)e * 3 + 2] + Jz[0] * R.ip[q * 3 + 0] +
+                         Jz[1] * R.ip[q * 3 + 1] + Jz[2] * R.ip[q * 3 + 2];
+        const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+        qtab[j] = pml_qcoef(pml, rule, rule == 0 ? mask_cc : mask_mass, z, R.w[q] * detJ[e], eps);
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // producers only
+      for (int rule = 0; rule < 2; ++rule) {
+        const int mask = rule == 0 ? mask_cc : mask_mass;
+        if (!mask) continue;
+        const Rule R = rule == 0 ? rcc : rm;
+        const QCoef *qc = qtab + (rule == 0 ? 0 : rcc.nq);
+        const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+        const bool need_v = rule == 1;
+        const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+        for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
+          const int nqc = min(QC, R.nq - q0);
+          const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
+          const unsigned b = c & 1u, use = c >> 1;
+          if (live) live = mbar_wait(&empty[b], (use & 1u) ^ 1u, err);
+          double *Xs = smem + b * Sh::BUF;
+          double *Yr = Xs + RMAX * LD;
+          double *Yi = Yr + RMAX * LD;
+          for (int i = ptid; i < (nrows4 - nrows) * LD; i += WS_PROD * 32) {
+            const int r = nrows + i / LD, k = i % LD;
+            Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+          }
+          for (int it = ptid; it < nqc * npair; it += WS_PROD * 32) {
+            const int qi = it / npair, pr = it - qi * npair;
+            pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, sJ, sJi,
+                               sidet, sfo, qc[q0 + qi], Xs, Yr, Yi);
+          }
+          mbar_arrive(&full[b]);
+        }
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // table free again
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int g = lane >> 2, t4 = lane & 3;
+  const int nt = warp % 6, mh = warp / 6;  // column tile, row-tile half
+  unsigned c = 0;
+  for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
+    const int e = list[ie];
+    double cr[3][2], ci[3][2];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
+    for (int rule = 0; rule < 2; ++rule) {
+      const int mask = rule == 0 ? mask_cc : mask_mass;
+      if (!mask) continue;
+      const Rule R = rule == 0 ? rcc : rm;
+      const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+      const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+      for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
+        const int nqc = min(QC, R.nq - q0);
+        const int nrows4 = (nqc * rq + 3) & ~3;
+        const unsigned b = c & 1u, use = c >> 1;
+        if (live) live = mbar_wait(&full[b], use & 1u, err);
+        const double *Xs = smem + b * Sh::BUF;
+        const double *Yr = Xs + RMAX * LD;
+        const double *Yi = Yr + RMAX * LD;
+        for (int r0 = 0; r0 < nrows4; r0 += 4) {
+          const double br = Yr[(r0 + t4) * LD + nt * 8 + g];
+          const double bi = Yi[(r0 + t4) * LD + nt * 8 + g];
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            const double a = Xs[(r0 + t4) * LD + (mh * 3 + m) * 8 + g];
+            dmma(cr[m][0], cr[m][1], a, br);
+            dmma(ci[m][0], ci[m][1], a, bi);
+          }
+        }
+        mbar_arrive(&empty[b]);
+      }
+    }
+    // epilogue: C[row = (3 mh + m) 8 + g][col = 8 nt + 2 t4 + i]
+    const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
+    const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+    dcplx *dst = Ae + (size_t)e * nd * rs;
+    const int col = nt * 8 + 2 * t4;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int row = (mh * 3 + m) * 8 + g;
       if (row >= nd) continue;
       dcplx v2[2];
 #pragma unroll

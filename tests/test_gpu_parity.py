@@ -245,6 +245,52 @@ def test_bulk_variants(kcase, variant):
     assert g.Tuning()[0] == variant
 
 
+PML_WS_CASES = [("grating", 3, 6.0), ("hole", 3, 0.0), ("slab", 3, 6.0), ("poly", 3, 6.0)]
+
+
+def _case_any(kind, p, theta):
+    if kind == "poly":
+        return configs.small_poly_case(p, theta, seed=5)
+    if kind == "slab":
+        return configs.small_case("slab", p, theta, seed=13, h=3.2)
+    return case(kind, p, theta)
+
+
+@pytest.mark.parametrize("kcase", PML_WS_CASES, ids=ids)
+def test_pml_ws_variant(kcase):
+    """The warp-specialised p = 3 PML kernel matches the oracle for every
+    integrator mask, with and without the transform, and assembled."""
+    c = _case_any(*kcase)
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(c.ad, 0) and g.SetPmlVariant(1)
+    assert g.PathCounts()[1] > 0
+    mm = MASS | ((CROSS0 | CROSS1 | KLK) if c.prob.has_kpar else 0)
+    masks = [(CURLCURL, mm, True), (CURLCURL, mm, False), (CURLCURL, 0, False), (0, MASS, False)]
+    if c.prob.has_kpar:
+        masks += [(0, CROSS0, False), (0, CROSS1, False), (0, KLK, False)]
+    for mcc, mmass, te in masks:
+        assert g.ComputeLocal(mcc, mmass, te)
+        assert rel(g.DownloadLocal(), oracle.local(c.ad, c.prob, mcc, mmass, te)) < TOL, (mcc, mmass)
+    assert g.BuildGlobal(c.ad.ess)
+    I, J = oracle.csr(c.ad)
+    for elim in (False, True):
+        assert g.Assemble(elim)
+        assert rel(g.DownloadValues(), oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, elim)) < TOL
+    assert g.PmlTuning()[0] == 1
+
+
+def test_pml_variant_selection():
+    c = case("grating", 3, 6.0)
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Autotune()
+    v, ms = g.PmlTuning()
+    assert v in (0, 1) and min(ms) > 0 and ms[v] == min(ms)
+    c2 = case("grating", 2, 6.0)
+    g2 = AsmGpu(c2.prob)
+    assert g2.Init(c2.ad, 0)
+    assert not g2.SetPmlVariant(1) and g2.last_error[0] == 3
+
+
 def test_autotuner_picks_a_variant():
     c = case("grating", 2, 6.0)
     g = AsmGpuGlobal(c.prob)
