@@ -389,14 +389,16 @@ def run_ours(a, rank, world, local, dist, torch):
     top = int(np.argmax(stages))
     if top == 1:
         ach = kern["pml"]["TFLOP/s"]
-        roof = {"kernel": "k_pml_mma", "what": "PML elements, FP64 quadrature contraction on DMMA",
+        roof = {"kernel": "k_pml_ws" if pml_tuning[0] == 1 else "k_pml_mma",
+                "what": "PML elements, FP64 quadrature contraction on DMMA",
                 "bound": "tensor",
                 "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
                 "peak_source": "measured in-run: cuBLAS DGEMM 8192^3", "traffic": None}
     else:
         nm = stage_names[top]
         ach = kern[nm]["GB/s"]
-        roof = {"kernel": {"prep+bulk": "k_bulk", "gather": "k_gather"}[nm], "bound": "hbm",
+        roof = {"kernel": {"prep+bulk": "k_bulk_mma" if tuning[0] else "k_bulk",
+                           "gather": "k_gather"}[nm], "bound": "hbm",
                 "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
     prof_path = ROOT / "profiles" / "traffic_c3_line_grating_p3.json"
