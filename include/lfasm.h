@@ -246,6 +246,28 @@ int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3);
 int lfasm_set_pml_variant(lfasm_handle *h, int variant);
 int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms2);
 
+/* Field sampling and the orders' adjoint seed (the reference samples planes
+ * with MFEM FindPoints/GetVectorValue, solver/lithofem_solve.cpp:951-1004,
+ * and takes orders by FFT, src/lithofem/orders.py:36-67).
+ * lfasm_set_basis hands over the element basis for evaluation away from the
+ * quadrature points: nmono monomials x^a y^b z^c (exps[3 m .. 3 m + 2],
+ * a + b + c <= p) and the coefficients of the nd functions and of their
+ * curls, coef[(k * 3 + d) * nmono + m] (component d of function k).
+ * lfasm_sample_plane: E and curl E of the device solution d_u (n
+ * complex128, global coefficients) at the points ((i + 1/2) lx / nx +
+ * 3.1e-7, (j + 1/2) ly / ny + 1.7e-7, z - 4.9e-7), j-major, into d_e and
+ * d_curl (ny * nx * 3 complex128 each, either may be NULL), as the
+ * reference's sampler; LFASM_ERR_ARG if a point lies outside the mesh.
+ * lfasm_plane_seed: d_c (n complex128, overwritten) with c^T u equal to the
+ * (m, q) Fourier coefficient (1 / (nx ny)) sum_{j,i} E_comp(x_ij)
+ * exp(-2 pi i (m i / nx + q j / ny)) of component comp of those samples. */
+int lfasm_set_basis(lfasm_handle *h, int nmono, const int *exps, const double *coef,
+                    const double *curl_coef);
+int lfasm_sample_plane(lfasm_handle *h, double lx, double ly, double z, int nx, int ny,
+                       const void *d_u, void *d_e, void *d_curl);
+int lfasm_plane_seed(lfasm_handle *h, double lx, double ly, double z, int nx, int ny, int comp,
+                     int m, int q, void *d_c);
+
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
  * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the

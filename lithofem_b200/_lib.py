@@ -71,6 +71,11 @@ def lib() -> ct.CDLL:
         "lfasm_get_pml_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
         "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
+        "lfasm_set_basis": (ct.c_int, [H, ct.c_int, c_int_p, c_double_p, c_double_p]),
+        "lfasm_sample_plane": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_double, ct.c_int,
+                                          ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+        "lfasm_plane_seed": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_double, ct.c_int,
+                                        ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p]),
         "lfasm_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
         "lfasm_batch_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
         "lfasm_batch_assemble": (ct.c_int, [ct.c_void_p, ct.c_int]),

@@ -117,6 +117,32 @@ class AsmGpu:
         _lib.check(_lib.lib().lfasm_get_pml_tuning(self._h, ct.byref(v), ms))
         return v.value, [float(x) for x in ms]
 
+    # -- field sampling (solver/lithofem_solve.cpp:951-1004) ---------------
+    def SetBasis(self, el) -> bool:
+        """Hand the element basis (ndbasis.NDElement) to the library."""
+        self._bexps = np.ascontiguousarray(np.asarray(el.monos, dtype=np.int32).reshape(-1))
+        self._bcoef = np.ascontiguousarray(el.coef, dtype=np.float64)
+        self._bccoef = np.ascontiguousarray(el._curl_coef, dtype=np.float64)
+        return self._ok(_lib.lib().lfasm_set_basis(
+            self._h, len(el.monos), self._bexps.ctypes.data_as(c_int_p),
+            self._bcoef.ctypes.data_as(c_double_p), self._bccoef.ctypes.data_as(c_double_p)))
+
+    def SamplePlane(self, lx: float, ly: float, z: float, nx: int, ny: int, u_ptr: int,
+                    e_ptr: int, curl_ptr: int = 0) -> bool:
+        """E (and curl E) of the device solution at the reference's plane grid,
+        [ny][nx][3] complex128 into e_ptr / curl_ptr (device)."""
+        return self._ok(_lib.lib().lfasm_sample_plane(
+            self._h, float(lx), float(ly), float(z), int(nx), int(ny), ct.c_void_p(u_ptr),
+            ct.c_void_p(e_ptr or None), ct.c_void_p(curl_ptr or None)))
+
+    def PlaneSeed(self, lx: float, ly: float, z: float, nx: int, ny: int, comp: int, m: int,
+                  q: int, c_ptr: int) -> bool:
+        """c (device, n complex128) with c^T u = the (m, q) Fourier coefficient
+        of component comp of the plane samples."""
+        return self._ok(_lib.lib().lfasm_plane_seed(
+            self._h, float(lx), float(ly), float(z), int(nx), int(ny), int(comp), int(m),
+            int(q), ct.c_void_p(c_ptr)))
+
     def PathCounts(self) -> tuple[int, int]:
         a, b = ct.c_int(), ct.c_int()
         _lib.check(_lib.lib().lfasm_path_counts(self._h, ct.byref(a), ct.byref(b)))

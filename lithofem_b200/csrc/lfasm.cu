@@ -216,6 +216,10 @@ struct lfasm_handle {
   int pml_forced = 0;
   float pml_ms[2] = {0.f, 0.f};
   int *err = nullptr;  // device error word of the bounded-wait kernels
+  // element basis for sampling away from the quadrature points
+  int nmono = 0;
+  int *bexps = nullptr;
+  double *bcoef = nullptr, *bccoef = nullptr;
   dcplx *Ae = nullptr;
   // RHS data
   int *slab_of = nullptr;
@@ -1419,6 +1423,130 @@ void lfasm_batch_destroy(lfasm_batch *b) {
   batch_free(b);
 }
 
+int lfasm_set_basis(lfasm_handle *h, int nmono, const int *exps, const double *coef,
+                    const double *curl_coef) {
+  if (!h || !exps || !coef || !curl_coef) return fail(LFASM_ERR_ARG, "NULL argument");
+  if (nmono <= 0 || nmono > BASIS_MAX_MONO)
+    return fail(LFASM_ERR_UNSUPPORTED, "%d monomials (at most %d)", nmono, BASIS_MAX_MONO);
+  for (int m = 0; m < nmono; ++m) {
+    const int a = exps[3 * m], b = exps[3 * m + 1], c = exps[3 * m + 2];
+    if (a < 0 || b < 0 || c < 0 || a + b + c > h->p)
+      return fail(LFASM_ERR_ARG, "monomial %d has exponents (%d,%d,%d) beyond degree %d", m, a, b,
+                  c, h->p);
+  }
+  LF_CUDA(cudaSetDevice(h->dev));
+  dfree(h->bexps); dfree(h->bcoef); dfree(h->bccoef);
+  const size_t nc = (size_t)h->nd * 3 * nmono;
+  LF_CUDA(upload(h->bexps, exps, (size_t)nmono * 3));
+  LF_CUDA(upload(h->bcoef, coef, nc));
+  LF_CUDA(upload(h->bccoef, curl_coef, nc));
+  h->nmono = nmono;
+  return LFASM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// locate the nx x ny sample points of the plane z: element and reference
+// coordinates per point (device arrays owned by the caller afterwards)
+int plane_locate(lfasm_handle *h, const PlaneGrid &G, int **elem, double **xi) {
+  const int ne = h->ne, npts = G.nx * G.ny;
+  int *flag = nullptr, *pos = nullptr, *cand = nullptr, *miss = nullptr;
+  unsigned char *tmp = nullptr;
+  size_t tb = 0;
+  LF_CUDA(dmalloc(flag, (size_t)ne + 1));
+  LF_CUDA(dmalloc(pos, (size_t)ne + 1));
+  LF_CUDA(dmalloc(cand, (size_t)ne));
+  LF_CUDA(dmalloc(miss, 1));
+  LF_CUDA(dmalloc(*elem, (size_t)npts));
+  LF_CUDA(dmalloc(*xi, (size_t)npts * 3));
+  LF_CUDA(cudaMemsetAsync(flag + ne, 0, sizeof(int), h->stream));
+  LF_CUDA(cudaMemsetAsync(miss, 0, sizeof(int), h->stream));
+  const unsigned gb = (unsigned)((ne + 255) / 256);
+  k_plane_cand<<<gb, 256, 0, h->stream>>>(ne, h->J, h->v0, G.z - 4.9e-7, flag);
+  LF_LAUNCHED();
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, ne + 1, h->stream));
+  LF_CUDA(dmalloc(tmp, tb));
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, pos, ne + 1, h->stream));
+  k_compact<<<gb, 256, 0, h->stream>>>(ne, flag, pos, cand);
+  LF_LAUNCHED();
+  int ncand = 0;
+  LF_CUDA(cudaMemcpyAsync(&ncand, pos + ne, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  const int wpb = 8;
+  k_plane_locate<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
+      G, ncand, cand, h->Jinv, h->v0, *elem, *xi, miss);
+  LF_LAUNCHED();
+  int nmiss = 0;
+  LF_CUDA(cudaMemcpyAsync(&nmiss, miss, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(flag); dfree(pos); dfree(cand); dfree(miss); dfree(tmp);
+  if (nmiss) {
+    dfree(*elem); dfree(*xi);
+    return fail(LFASM_ERR_ARG, "%d of %d sample points of the plane z = %g lie outside the mesh",
+                nmiss, npts, G.z);
+  }
+  return LFASM_OK;
+}
+
+int plane_args(lfasm_handle *h, double lx, double ly, double z, int nx, int ny, PlaneGrid &G) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (!h->nmono) return fail(LFASM_ERR_STATE, "lfasm_set_basis has not run");
+  if (nx <= 0 || ny <= 0 || (long long)nx * ny > (1ll << 24) || !(lx > 0) || !(ly > 0))
+    return fail(LFASM_ERR_ARG, "bad sampling grid %d x %d over %g x %g", nx, ny, lx, ly);
+  G.lx = lx; G.ly = ly; G.z = z; G.nx = nx; G.ny = ny;
+  return LFASM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfasm_sample_plane(lfasm_handle *h, double lx, double ly, double z, int nx, int ny,
+                       const void *d_u, void *d_e, void *d_curl) {
+  PlaneGrid G;
+  int rc = plane_args(h, lx, ly, z, nx, ny, G);
+  if (rc) return rc;
+  if (!d_u || (!d_e && !d_curl)) return fail(LFASM_ERR_ARG, "NULL vector");
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(h->dev));
+  int *elem = nullptr;
+  double *xi = nullptr;
+  if ((rc = plane_locate(h, G, &elem, &xi))) return rc;
+  const int npts = nx * ny, wpb = 8;
+  k_plane_eval<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
+      npts, elem, xi, h->nd, h->p, h->nmono, h->bexps, h->bcoef, h->bccoef, h->dof, h->sign,
+      h->fopack, h->J, h->Jinv, h->detJ, (const dcplx *)d_u, (dcplx *)d_e, (dcplx *)d_curl);
+  LF_LAUNCHED();
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(elem); dfree(xi);
+  return sync_if(h);
+}
+
+int lfasm_plane_seed(lfasm_handle *h, double lx, double ly, double z, int nx, int ny, int comp,
+                     int m, int q, void *d_c) {
+  PlaneGrid G;
+  int rc = plane_args(h, lx, ly, z, nx, ny, G);
+  if (rc) return rc;
+  if (!d_c) return fail(LFASM_ERR_ARG, "NULL vector");
+  if (comp < 0 || comp > 2) return fail(LFASM_ERR_ARG, "component %d outside 0..2", comp);
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(h->dev));
+  int *elem = nullptr;
+  double *xi = nullptr;
+  if ((rc = plane_locate(h, G, &elem, &xi))) return rc;
+  const int npts = nx * ny, wpb = 8;
+  LF_CUDA(cudaMemsetAsync(d_c, 0, (size_t)h->n * sizeof(dcplx), h->stream));
+  k_plane_seed<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
+      G, elem, xi, h->nd, h->p, h->nmono, h->bexps, h->bcoef, h->bccoef, h->dof, h->sign,
+      h->fopack, h->J, h->Jinv, h->detJ, comp, m, q, (double *)d_c);
+  LF_LAUNCHED();
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(elem); dfree(xi);
+  return sync_if(h);
+}
+
 int lfasm_set_profile(lfasm_handle *h, int on) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   LF_CUDA(cudaSetDevice(h->dev));
@@ -1720,7 +1848,7 @@ void lfasm_destroy(lfasm_handle *h) {
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
   for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
-  dfree(h->S); dfree(h->err); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
+  dfree(h->S); dfree(h->err); dfree(h->bexps); dfree(h->bcoef); dfree(h->bccoef); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);
   dfree(h->ess); dfree(h->ea_ptr); dfree(h->ea); dfree(h->long_rows); dfree(h->off); dfree(h->partials);
   dfree(h->red);

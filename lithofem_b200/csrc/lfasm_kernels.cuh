@@ -1774,4 +1774,226 @@ __global__ void k_eps_grad(int nsel, const int *__restrict__ list, int nd, int p
   }
 }
 
+// ---------------------------------------------------------------------------
+// Field sampling on a z-plane (the reference's plane sampler,
+// solver/lithofem_solve.cpp:951-1004) and the adjoint seed of one Fourier
+// order of the samples (src/lithofem/orders.py:36-67).
+// ---------------------------------------------------------------------------
+constexpr int BASIS_MAX_MONO = 20;  // monomials of degree <= 3
+
+struct PlaneGrid {
+  double lx, ly, z;
+  int nx, ny;
+};
+
+// sample point (i, j): cell-centred with the reference's fixed nudges
+__device__ __forceinline__ void plane_point(const PlaneGrid &G, int pt, double x[3]) {
+  const int i = pt % G.nx, j = pt / G.nx;
+  x[0] = (i + 0.5) * G.lx / G.nx + 3.1e-7;
+  x[1] = (j + 0.5) * G.ly / G.ny + 1.7e-7;
+  x[2] = G.z - 4.9e-7;
+}
+
+// elements whose z-range contains z (vertex z = v0z + J20 / J21 / J22)
+__global__ void k_plane_cand(int ne, const double *__restrict__ J9, const double *__restrict__ v0,
+                             double z, int *__restrict__ flag) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const double z0 = v0[(size_t)e * 3 + 2];
+  double lo = z0, hi = z0;
+  for (int c = 0; c < 3; ++c) {
+    const double zc = z0 + J9[(size_t)e * 9 + 6 + c];
+    lo = fmin(lo, zc);
+    hi = fmax(hi, zc);
+  }
+  const double tol = 1e-9 * (1.0 + fabs(z));
+  flag[e] = (z >= lo - tol && z <= hi + tol) ? 1 : 0;
+}
+
+__global__ void k_compact(int n, const int *__restrict__ flag, const int *__restrict__ pos,
+                          int *__restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n && flag[e]) out[pos[e]] = e;
+}
+
+// one warp per sample point: the candidate element in which the point is
+// most interior (largest smallest barycentric coordinate; lower index on a
+// tie) and the point's reference coordinates; *missing counts points that
+// lie outside every candidate
+__global__ void k_plane_locate(PlaneGrid G, int ncand, const int *__restrict__ cand,
+                               const double *__restrict__ Ji9, const double *__restrict__ v0,
+                               int *__restrict__ elem, double *__restrict__ xi,
+                               int *__restrict__ missing) {
+  const int lane = threadIdx.x & 31;
+  const int pt = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pt >= G.nx * G.ny) return;
+  double x[3];
+  plane_point(G, pt, x);
+  double best = -1e300;
+  int be = 0x7fffffff;
+  for (int i = lane; i < ncand; i += 32) {
+    const int e = cand[i];
+    const double *Ji = Ji9 + (size_t)e * 9;
+    const double d0 = x[0] - v0[(size_t)e * 3], d1 = x[1] - v0[(size_t)e * 3 + 1],
+                 d2 = x[2] - v0[(size_t)e * 3 + 2];
+    const double a = Ji[0] * d0 + Ji[1] * d1 + Ji[2] * d2;
+    const double b = Ji[3] * d0 + Ji[4] * d1 + Ji[5] * d2;
+    const double c = Ji[6] * d0 + Ji[7] * d1 + Ji[8] * d2;
+    const double m = fmin(fmin(1.0 - a - b - c, a), fmin(b, c));
+    if (m > best || (m == best && e < be)) { best = m; be = e; }
+  }
+  for (int o = 16; o; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oe = __shfl_xor_sync(0xffffffffu, be, o);
+    if (ob > best || (ob == best && oe < be)) { best = ob; be = oe; }
+  }
+  if (lane == 0) {
+    if (be == 0x7fffffff || best < -1e-9) {
+      atomicAdd(missing, 1);
+      elem[pt] = -1;
+      return;
+    }
+    elem[pt] = be;
+    const double *Ji = Ji9 + (size_t)be * 9;
+    const double d0 = x[0] - v0[(size_t)be * 3], d1 = x[1] - v0[(size_t)be * 3 + 1],
+                 d2 = x[2] - v0[(size_t)be * 3 + 2];
+    xi[pt * 3 + 0] = Ji[0] * d0 + Ji[1] * d1 + Ji[2] * d2;
+    xi[pt * 3 + 1] = Ji[3] * d0 + Ji[4] * d1 + Ji[5] * d2;
+    xi[pt * 3 + 2] = Ji[6] * d0 + Ji[7] * d1 + Ji[8] * d2;
+  }
+}
+
+// Global basis functions of element e at reference point xi for the pair of
+// local functions (2 pr, 2 pr + 1): physical values psi (covariant map,
+// v J^-1) and physical curls (J c / detJ), with the face transform applied
+// like in the element kernels.  k >= nd gives zeros.
+__device__ __forceinline__ void basis_pair(int e, int pr, const double *xi, int nd, int p,
+                                           int nmono, const int *__restrict__ exps,
+                                           const double *__restrict__ coef,
+                                           const double *__restrict__ ccoef,
+                                           const double *__restrict__ J9,
+                                           const double *__restrict__ Ji9,
+                                           const double *__restrict__ detJ, unsigned fo,
+                                           double v[2][3], double c[2][3]) {
+  double mono[BASIS_MAX_MONO];
+  for (int m = 0; m < nmono; ++m) {
+    double t = 1.0;
+    for (int a = 0; a < exps[3 * m + 0]; ++a) t *= xi[0];
+    for (int a = 0; a < exps[3 * m + 1]; ++a) t *= xi[1];
+    for (int a = 0; a < exps[3 * m + 2]; ++a) t *= xi[2];
+    mono[m] = t;
+  }
+  const double *J = J9 + (size_t)e * 9, *Ji = Ji9 + (size_t)e * 9;
+  const double idet = 1.0 / detJ[e];
+  for (int h = 0; h < 2; ++h) {
+    const int k = 2 * pr + h;
+    double r[3] = {0.0, 0.0, 0.0}, q[3] = {0.0, 0.0, 0.0};
+    if (k < nd)
+      for (int d = 0; d < 3; ++d)
+        for (int m = 0; m < nmono; ++m) {
+          r[d] += coef[((size_t)k * 3 + d) * nmono + m] * mono[m];
+          q[d] += ccoef[((size_t)k * 3 + d) * nmono + m] * mono[m];
+        }
+    for (int d = 0; d < 3; ++d) {
+      v[h][d] = r[0] * Ji[0 * 3 + d] + r[1] * Ji[1 * 3 + d] + r[2] * Ji[2 * 3 + d];
+      c[h][d] = (J[d * 3 + 0] * q[0] + J[d * 3 + 1] * q[1] + J[d * 3 + 2] * q[2]) * idet;
+    }
+  }
+  if (p >= 2) {
+    const int f = face_of(2 * pr, p);
+    if (f >= 0) {
+      const double *T = c_tinv + 4 * ((fo >> (8 * f)) & 0xffu);
+      for (int d = 0; d < 3; ++d) {
+        const double v0_ = v[0][d], v1_ = v[1][d], c0_ = c[0][d], c1_ = c[1][d];
+        v[0][d] = v0_ * T[0] + v1_ * T[1];
+        v[1][d] = v0_ * T[2] + v1_ * T[3];
+        c[0][d] = c0_ * T[0] + c1_ * T[1];
+        c[1][d] = c0_ * T[2] + c1_ * T[3];
+      }
+    }
+  }
+}
+
+// one warp per sample point: E and curl E of u (global coefficients, dof
+// signs) at the located point; out layout [pt][3] complex
+__global__ void k_plane_eval(int npts, const int *__restrict__ elem, const double *__restrict__ xi,
+                             int nd, int p, int nmono, const int *__restrict__ exps,
+                             const double *__restrict__ coef, const double *__restrict__ ccoef,
+                             const int *__restrict__ dof, const double *__restrict__ sign,
+                             const unsigned *__restrict__ fopack, const double *__restrict__ J9,
+                             const double *__restrict__ Ji9, const double *__restrict__ detJ,
+                             const dcplx *__restrict__ u, dcplx *__restrict__ E,
+                             dcplx *__restrict__ curlE) {
+  const int lane = threadIdx.x & 31;
+  const int pt = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pt >= npts) return;
+  const int e = elem[pt];
+  double acc[12];
+  for (int i = 0; i < 12; ++i) acc[i] = 0.0;
+  const int npair = (nd + 1) / 2;
+  if (e >= 0 && lane < npair) {
+    double v[2][3], c[2][3];
+    basis_pair(e, lane, xi + (size_t)pt * 3, nd, p, nmono, exps, coef, ccoef, J9, Ji9, detJ,
+               fopack[e], v, c);
+    for (int h = 0; h < 2; ++h) {
+      const int k = 2 * lane + h;
+      if (k >= nd) continue;
+      const dcplx g = u[dof[(size_t)e * nd + k]];
+      const double s = sign[(size_t)e * nd + k];
+      for (int d = 0; d < 3; ++d) {
+        acc[2 * d] += s * g.re * v[h][d];
+        acc[2 * d + 1] += s * g.im * v[h][d];
+        acc[6 + 2 * d] += s * g.re * c[h][d];
+        acc[6 + 2 * d + 1] += s * g.im * c[h][d];
+      }
+    }
+  }
+  for (int i = 0; i < 12; ++i)
+    for (int o = 16; o; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+  if (lane == 0) {
+    for (int d = 0; d < 3; ++d) {
+      if (E) E[(size_t)pt * 3 + d] = mk(acc[2 * d], acc[2 * d + 1]);
+      if (curlE) curlE[(size_t)pt * 3 + d] = mk(acc[6 + 2 * d], acc[6 + 2 * d + 1]);
+    }
+  }
+}
+
+// adjoint seed of the (m, q) Fourier coefficient of component comp of the
+// sampled E: c[dof_k] += sign_k psi_k(x_pt)[comp] exp(-2 pi i (m i/nx + q j/ny)) / (nx ny)
+__global__ void k_plane_seed(PlaneGrid G, const int *__restrict__ elem,
+                             const double *__restrict__ xi, int nd, int p, int nmono,
+                             const int *__restrict__ exps, const double *__restrict__ coef,
+                             const double *__restrict__ ccoef, const int *__restrict__ dof,
+                             const double *__restrict__ sign, const unsigned *__restrict__ fopack,
+                             const double *__restrict__ J9, const double *__restrict__ Ji9,
+                             const double *__restrict__ detJ, int comp, int m, int q,
+                             double *__restrict__ cvec) {
+  const int lane = threadIdx.x & 31;
+  const int npts = G.nx * G.ny;
+  const int pt = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pt >= npts) return;
+  const int e = elem[pt];
+  const int npair = (nd + 1) / 2;
+  if (e < 0 || lane >= npair) return;
+  const int i = pt % G.nx, j = pt / G.nx;
+  // phase -2 pi (m i / nx + q j / ny), reduced to one period first
+  const long long num = ((long long)m * i * G.ny + (long long)q * j * G.nx) %
+                        ((long long)G.nx * G.ny);
+  const double ang = -2.0 * 3.141592653589793238 * (double)num / ((double)G.nx * G.ny);
+  double sn, cs;
+  sincos(ang, &sn, &cs);
+  const double inv = 1.0 / npts;
+  double v[2][3], c[2][3];
+  basis_pair(e, lane, xi + (size_t)pt * 3, nd, p, nmono, exps, coef, ccoef, J9, Ji9, detJ,
+             fopack[e], v, c);
+  for (int h = 0; h < 2; ++h) {
+    const int k = 2 * lane + h;
+    if (k >= nd) continue;
+    const double w = sign[(size_t)e * nd + k] * v[h][comp] * inv;
+    double *dst = cvec + 2 * (size_t)dof[(size_t)e * nd + k];
+    atomicAdd(dst, w * cs);
+    atomicAdd(dst + 1, w * sn);
+  }
+}
+
 }  // namespace lfasm_dev

@@ -1,0 +1,85 @@
+"""Diffraction orders and order efficiencies from plane samples.
+
+Restates the reference's post-processing: ``orders_from_plane`` (FFT of the
+(ny, nx, 3) envelope samples, src/lithofem/orders.py:36-67),
+``one_way_flux_z`` (:70-86) and the order efficiency of a one-way region
+with the analytic (0,0) background term (src/lithofem/outputs.py:219-269).
+The samples come from ``lfasm_sample_plane``; the adjoint seed of one
+order's coefficient from ``lfasm_plane_seed``.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass(frozen=True)
+class OrderSet:
+    """Per-order envelope coefficients on a z-plane and their wavevectors."""
+
+    ms: np.ndarray
+    ns: np.ndarray
+    coeffs: np.ndarray    # (n, 3) complex
+    kx: np.ndarray
+    ky: np.ndarray
+    qz: np.ndarray        # complex, Im >= 0
+    k0: float
+    eps: complex
+
+
+def order_qz(k0: float, eps: complex, kx: float, ky: float) -> complex:
+    qz = np.sqrt(complex(k0 ** 2 * eps - kx ** 2 - ky ** 2))
+    return -qz if qz.imag < 0 else qz
+
+
+def orders_from_plane(u: np.ndarray, lx: float, ly: float, kpar: tuple[float, float],
+                      k0: float, eps_medium: complex) -> OrderSet:
+    """FFT the (ny, nx, 3) envelope samples into Fourier orders."""
+    ny, nx, _ = u.shape
+    c = np.fft.fft2(u, axes=(0, 1)) / (nx * ny)
+    gx, gy = 2 * np.pi / lx, 2 * np.pi / ly
+    ms, ns, coeffs, kxs, kys, qzs = [], [], [], [], [], []
+    for j in range(ny):
+        n_idx = j if j <= ny // 2 else j - ny
+        for i in range(nx):
+            m_idx = i if i <= nx // 2 else i - nx
+            kx = kpar[0] + gx * m_idx
+            ky = kpar[1] + gy * n_idx
+            ms.append(m_idx)
+            ns.append(n_idx)
+            coeffs.append(c[j, i])
+            kxs.append(kx)
+            kys.append(ky)
+            qzs.append(order_qz(k0, eps_medium, kx, ky))
+    return OrderSet(ms=np.array(ms), ns=np.array(ns), coeffs=np.array(coeffs),
+                    kx=np.array(kxs), ky=np.array(kys), qz=np.array(qzs), k0=k0,
+                    eps=complex(eps_medium))
+
+
+def plane_wave_flux(c: np.ndarray, kx: float, ky: float, qz: complex, k0: float,
+                    direction: int, area: float) -> float:
+    """z-power of one plane-wave order: Re[(E x (k x E / k0)*)_z] / 2 x area."""
+    k = np.array([kx, ky, direction * qz])
+    h = np.cross(k, c) / k0
+    return 0.5 * float(np.real(np.cross(c, np.conj(h))[2])) * area
+
+
+def one_way_flux_z(orders: OrderSet, direction: int, area: float) -> float:
+    return sum(plane_wave_flux(orders.coeffs[i], orders.kx[i], orders.ky[i], orders.qz[i],
+                               orders.k0, direction, 1.0) for i in range(len(orders.ms))) * area
+
+
+def zeroth_order_efficiency(c00: np.ndarray, z: float, z_ref: float, kpar, k0: float,
+                            eps_medium: complex, eps_in: complex, amp00: complex,
+                            e_bg: np.ndarray, lx: float, ly: float, direction: int = 1) -> float:
+    """Efficiency of the (0,0) order on the reflection (+1) or transmission
+    (-1) side: the scattered coefficient c00 propagated to the reference
+    plane z_ref, plus the analytic background amp00 e_bg, as a flux over the
+    incident flux (outputs.py:219-269)."""
+    qz = order_qz(k0, eps_medium, kpar[0], kpar[1])
+    c = c00 * np.exp(-1j * direction * qz * (z - z_ref)) + amp00 * e_bg
+    qz_in = np.sqrt(complex(k0 ** 2 * eps_in - kpar[0] ** 2 - kpar[1] ** 2))
+    inc_flux = 0.5 * (qz_in.real / k0) * lx * ly
+    return direction * plane_wave_flux(c, kpar[0], kpar[1], qz, k0, direction, lx * ly) / inc_flux
