@@ -119,6 +119,99 @@ class EpsAdjoint:
         return ell, abs(ell) ** 2, dJ_re, dJ_im, dl
 
 
+class EffAdjoint:
+    """The zeroth up-going order efficiency on a plane above the structure
+    and its gradient with respect to per-element eps.
+
+    eta = flux(c) / incident flux, c = the (0,0) Fourier coefficient of the
+    scattered envelope sampled on the plane (three component seeds from
+    lfasm_plane_seed, c_d = s_d^T u) plus the analytic reflected background
+    at the same plane (the up-going part of the top slab's incident table);
+    flux(c) = Re[(c x (k x c / k0)*)_z] / 2 x area with k = (kx, ky, qz) of
+    the order (outputs.py:219-269, orders.py:70-86).  As a real quadratic
+    form eta = kappa c^H Q c, so with g = kappa Q c the adjoint seed is
+    sum_d conj(g_d) s_d and deta/deps_e = 2 Re / -2 Im of
+    lambda^T (db/deps_e - dA/deps_e u) (lfasm_eps_gradient).
+    """
+
+    def __init__(self, ad, prob, parts, z_plane: float, lx: float, ly: float, nx: int = 8,
+                 ny: int = 8, gpu_id: int = 0, solver=HostLU):
+        self.ad, self.prob0, self.parts = ad, prob, parts
+        self.z, self.lx, self.ly, self.nx, self.ny = z_plane, lx, ly, nx, ny
+        self.gpu_id, self.solver_cls = gpu_id, solver
+        k0 = prob.k0
+        kx, ky = prob.kx, prob.ky
+        # top-slab incident tables of every part (one plane wave's s/p parts
+        # share the direction): A down-going incident, B up-going background
+        tops = [part[-1] for part in parts]
+        qz = tops[0].qB
+        self.k = np.array([kx, ky, qz.real])
+        self.k0 = k0
+        self.c_bg = sum(t.B * np.exp(1j * t.qB * (z_plane - t.zB)) for t in tops)
+        a_in = sum(t.A * np.exp(1j * t.qA * (z_plane - t.zA)) for t in tops)
+        self.area = lx * ly
+        self.inc_flux = abs(self._flux(a_in, np.array([kx, ky, tops[0].qA.real])))
+        self._seeds = None
+
+    def _flux(self, c, k) -> float:
+        h = np.cross(k, c) / self.k0
+        return 0.5 * float(np.real(np.cross(c, np.conj(h))[2])) * self.area
+
+    def _Q(self) -> np.ndarray:
+        kx, ky, kz = self.k
+        return np.array([[kz, 0.0, -kx / 2], [0.0, kz, -ky / 2], [-kx / 2, -ky / 2, 0.0]])
+
+    def _assemble(self, eps):
+        import torch
+        prob = copy.copy(self.prob0)
+        prob.elem_eps = np.asarray(eps, dtype=complex)
+        g = AsmGpuGlobal(prob)
+        assert g.Init(self.ad, self.gpu_id) and g.BuildGlobal(self.ad.ess) and g.Assemble(True)
+        dev = f"cuda:{self.gpu_id}"
+        b = torch.zeros(self.ad.height, dtype=torch.complex128, device=dev)
+        assert g.AssembleRHS(self.parts, [0] * len(self.parts), 1, True, b.data_ptr())
+        if self._seeds is None:
+            assert g.SetBasis(ndbasis.nd_element(self.ad.p))
+            seeds = []
+            for comp in range(3):
+                sd = torch.empty(self.ad.height, dtype=torch.complex128, device=dev)
+                assert g.PlaneSeed(self.lx, self.ly, self.z, self.nx, self.ny, comp, 0, 0,
+                                   sd.data_ptr())
+                seeds.append(sd.cpu().numpy())
+            self._seeds = np.stack(seeds)
+        return g, b
+
+    def coefficient(self, u: np.ndarray) -> np.ndarray:
+        return self._seeds @ u + self.c_bg
+
+    def efficiency(self, c: np.ndarray) -> float:
+        return self._flux(c, self.k) / self.inc_flux
+
+    def value(self, eps) -> float:
+        g, b = self._assemble(eps)
+        u = self.solver_cls(g).solve(b.cpu().numpy())
+        return self.efficiency(self.coefficient(u))
+
+    def value_and_grad(self, eps):
+        """(eta, deta/dRe eps, deta/dIm eps) for eps (ne complex)."""
+        import torch
+        g, b = self._assemble(eps)
+        lu = self.solver_cls(g)
+        u = lu.solve(b.cpu().numpy())
+        c = self.coefficient(u)
+        eta = self.efficiency(c)
+        kappa = 0.5 * self.area / (self.k0 * self.inc_flux)
+        gw = kappa * (self._Q() @ c)
+        lam = lu.solve_transposed(np.conj(gw) @ self._seeds)
+        dev = b.device
+        ud = torch.from_numpy(u).to(dev)
+        ld = torch.from_numpy(lam).to(dev)
+        gd = torch.zeros(self.ad.ne, dtype=torch.complex128, device=dev)
+        assert g.EpsGradient(self.parts, ud.data_ptr(), ld.data_ptr(), gd.data_ptr())
+        dl = gd.cpu().numpy()
+        return eta, 2.0 * np.real(dl), -2.0 * np.imag(dl)
+
+
 def autograd_function(adj: EpsAdjoint):
     """torch.autograd.Function mapping (Re eps, Im eps) -> J = |l|^2."""
     import torch

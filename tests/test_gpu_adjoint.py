@@ -113,3 +113,51 @@ def test_autograd_function_backward():
     _, J2, gre, gim, _ = adj.value_and_grad(pr.elem_eps)
     assert abs(float(J) - J2) <= 1e-12 * J2
     assert np.allclose(er.grad.numpy(), gre) and np.allclose(ei.grad.numpy(), gim)
+
+
+def test_efficiency_gradient_matches_central_fd_on_20_elements():
+    """The zeroth up-order efficiency (the contact-hole objective) from the
+    GPU plane seeds, and its adjoint gradient vs central FD (step 1e-6)."""
+    st, ad, pr, parts = _hole_case()
+    adj = adjoint.EffAdjoint(ad, pr, parts, z_plane=21.0, lx=st.lx, ly=st.ly, nx=8, ny=8)
+    eta, gre, gim = adj.value_and_grad(pr.elem_eps)
+    assert 0.0 < eta < 1.0
+    rng = np.random.default_rng(configs.SEED)
+    is_pml = np.array([pr.regions[a - 1].is_pml for a in ad.attr])
+    els = rng.choice(np.nonzero(~is_pml)[0], size=20, replace=False)
+    scale = max(np.abs(gre).max(), np.abs(gim).max())
+    h = 1e-6
+    worst = 0.0
+    for e in els:
+        for comp, an in ((1.0, gre[e]), (1j, gim[e])):
+            ep = pr.elem_eps.copy()
+            em = pr.elem_eps.copy()
+            ep[e] += h * comp
+            em[e] -= h * comp
+            fd = (adj.value(ep) - adj.value(em)) / (2 * h)
+            worst = max(worst, abs(fd - an) / scale)
+    assert worst < 1e-5, worst
+
+
+def test_bare_slab_zeroth_order_efficiency_is_the_tmm_reflectance():
+    """Without contrast the scattered field vanishes and the (0,0)
+    efficiency is the stack's reflectance |r|^2 (s polarisation)."""
+    from lithofem_b200 import tmm
+    st = mesh.Stack(lx=8.0, ly=8.0, z_min=0.0, z_max=24.0, wavelength=configs.WAVELENGTH,
+                    layers=[(0.0, 12.0, configs.ABSORBER)])
+    theta = 6.0
+    ms = mesh.build_mesh(st, 2.5)
+    pr = problem.Problem.from_stack(st, 2, incident.kpar_of(st, theta))
+    ad = space.build_asm_data(ms, 2, pr, local_order_seed=3)
+    parts = [incident.planewave_parts(st, theta, 0.0, "s")]
+    eps = pr.eps_table()[ad.attr - 1].copy()
+    adj = adjoint.EffAdjoint(ad, pr, parts, z_plane=20.0, lx=st.lx, ly=st.ly, nx=4, ny=4)
+    eta = adj.value(eps)
+    slabs = st.slabs
+    eps_s = [st.eps_bg_of_slab(i) for i in range(len(slabs) - 1)]
+    d = [slabs[i + 1] - slabs[i] for i in range(len(slabs) - 1)]
+    kx, ky = incident.kpar_of(st, theta)
+    res = tmm.solve(tmm.Stack(eps_in=eps_s[-1], eps_out=eps_s[0], eps=tuple(reversed(eps_s)),
+                              d=tuple(reversed(d))), st.wavelength, kpar=float(np.hypot(kx, ky)),
+                    pol="s")
+    assert abs(eta - abs(res.r) ** 2) < 1e-10, (eta, abs(res.r) ** 2)
