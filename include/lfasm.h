@@ -40,7 +40,10 @@ enum {
   LFASM_ERR_CUDA = 2,        /* CUDA runtime error                         */
   LFASM_ERR_UNSUPPORTED = 3, /* outside the supported envelope (p > 3 ...) */
   LFASM_ERR_STATE = 4,       /* call order (e.g. scatter before build)     */
-  LFASM_ERR_CSR = 5          /* given sparsity misses an element coupling  */
+  LFASM_ERR_CSR = 5,         /* given sparsity misses an element coupling  */
+  LFASM_ERR_INJECTED = 6     /* failure injected on the host: the variable
+                                LITHOFEM_ASM_FORCE_FAIL is set (the
+                                reference's switch, lithofem_solve.cpp:757-762) */
 };
 
 /* Integrator selection bits, identical to the reference's mask enum

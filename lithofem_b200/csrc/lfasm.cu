@@ -18,6 +18,7 @@
 #include <mutex>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -471,6 +472,12 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
   g_err.clear();
   if (!out) return fail(LFASM_ERR_ARG, "out handle pointer is NULL");
   *out = nullptr;
+  const char *inject = std::getenv("LITHOFEM_ASM_FORCE_FAIL");
+  if (inject && inject[0]) {
+    std::printf("asm_gpu: forced failure injected (LITHOFEM_ASM_FORCE_FAIL)\n");
+    std::fflush(stdout);
+    return fail(LFASM_ERR_INJECTED, "forced failure injected (LITHOFEM_ASM_FORCE_FAIL)");
+  }
   if (!ad || !prob) return fail(LFASM_ERR_ARG, "NULL asm data or problem");
   if (ad->ne <= 0) return fail(LFASM_ERR_ARG, "empty mesh (ne = %d)", ad->ne);
   if (ad->p < 1 || ad->p > 3)

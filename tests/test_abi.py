@@ -85,3 +85,17 @@ def test_validation_reports_the_first_offending_entry():
     fo[[11, 3]] = [6, -1]
     rc, msg = _init_with(c, fo=fo)
     assert rc == 1 and msg == "fo[3] = -1 outside 0..5"
+
+
+def test_injected_failure(monkeypatch, capfd):
+    """LITHOFEM_ASM_FORCE_FAIL (the reference's host-side switch,
+    solver/lithofem_solve.cpp:757-762) makes lfasm_init fail before any
+    other work, with the reference's log line."""
+    c = configs.small_case("slab", 1, 0.0)
+    m = _abi.marshal(c.ad, c.prob)
+    h = ct.c_void_p()
+    monkeypatch.setenv("LITHOFEM_ASM_FORCE_FAIL", "1")
+    rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
+    assert rc == 6 and not h.value
+    assert b"LITHOFEM_ASM_FORCE_FAIL" in _lib.lib().lfasm_last_error()
+    assert "asm_gpu: forced failure injected (LITHOFEM_ASM_FORCE_FAIL)" in capfd.readouterr().out
