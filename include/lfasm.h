@@ -285,6 +285,11 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml);
 
 void lfasm_destroy(lfasm_handle *h);
 
+/* 1 in the bounds-checked debug build (liblfasm_bounds.so, compiled with
+ * -DLFASM_BOUNDS: device index checks in the gather record a failure,
+ * skip the access and make the call return LFASM_ERR_CUDA), else 0. */
+int lfasm_bounds_checked(void);
+
 /* Batched assembly of several meshes on one device (the reference assembles
  * one mesh per process; no counterpart).  lfasm_batch_create takes n built
  * handles (lfasm_build_global done) of one device; they must outlive the

@@ -13,6 +13,10 @@ from pathlib import Path
 from ._abi import AsmDataC, IncidentPartC, ProblemC, c_double_p, c_int_p
 
 LIB_PATH = Path(__file__).resolve().parent / "liblfasm.so"
+# LFASM_LIBRARY selects another build of the same library (the
+# bounds-checked liblfasm_bounds.so); the default is the in-tree liblfasm.so
+if os.environ.get("LFASM_LIBRARY"):
+    LIB_PATH = Path(os.environ["LFASM_LIBRARY"]).resolve()
 
 _lib = None
 
@@ -71,6 +75,7 @@ def lib() -> ct.CDLL:
         "lfasm_get_pml_tuning": (ct.c_int, [H, c_int_p, ct.POINTER(ct.c_float)]),
         "lfasm_destroy": (None, [H]),
         "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
+        "lfasm_bounds_checked": (ct.c_int, []),
         "lfasm_set_basis": (ct.c_int, [H, ct.c_int, c_int_p, c_double_p, c_double_p]),
         "lfasm_sample_plane": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_double, ct.c_int,
                                           ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),

@@ -112,16 +112,20 @@ def poly_hole_stack(rng: np.random.Generator, lx: float = 96.0, ly: float = 96.0
     return st
 
 
-def batch_config(scale: float = 1.0, n: int = 16, seed: int = SEED, theta: float = 6.0
-                 ) -> list[Case]:
+def batch_config(scale: float = 1.0, n: int = 16, seed: int = SEED, theta: float = 6.0,
+                 only: list[int] | None = None) -> list[Case]:
     """The batched workload: n seeded polygon-hole meshes, p cycled 1, 2, 3,
-    DOF targets log-uniform in [20k, 400k] (times scale)."""
+    DOF targets log-uniform in [20k, 400k] (times scale).  ``only`` builds a
+    subset (one rank's share); the parameters of every mesh are still drawn
+    in sequence, so mesh i is the same whichever subset is built."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
         p = 1 + i % 3
         ndof = float(np.exp(rng.uniform(np.log(20e3), np.log(400e3)))) * scale
         st = poly_hole_stack(rng)
+        if only is not None and i not in only:
+            continue
         hole = st.frustums[0]
         name = (f"C5[{i}] polygon hole nv={len(hole.verts)} alpha={hole.alpha:.1f} "
                 f"t={hole.h:.1f} p={p}")

@@ -254,10 +254,27 @@ struct lfasm_handle {
 
 namespace {
 
+// bounds-checked build: the first failed device index check, if any
+int bounds_status() {
+#ifdef LFASM_BOUNDS
+  int e = 0;
+  LF_CUDA(cudaMemcpyFromSymbol(&e, g_bounds_err, sizeof(int)));
+  if (e) {
+    const int zero = 0;
+    LF_CUDA(cudaMemcpyToSymbol(g_bounds_err, &zero, sizeof(int)));
+    return fail(LFASM_ERR_CUDA, "device bounds check %d failed (%s)", e,
+                e == BOUNDS_SLOT ? "slot offset outside its CSR row"
+                                 : "row-list entry outside the element buffer");
+  }
+#endif
+  return LFASM_OK;
+}
+
 int sync_if(lfasm_handle *h) {
   LF_CUDA(cudaGetLastError());
   if (!h->async_mode) {
     LF_CUDA(cudaStreamSynchronize(h->stream));
+    if (int rb = bounds_status()) return rb;
     if (h->pml_variant == 1 && h->err) {
       int e = 0;
       LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -466,6 +483,14 @@ extern "C" {
 const char *lfasm_last_error(void) { return g_err.c_str(); }
 
 long long lfasm_launch_count(void) { return g_launches.load(); }
+
+int lfasm_bounds_checked(void) {
+#ifdef LFASM_BOUNDS
+  return 1;
+#else
+  return 0;
+#endif
+}
 
 int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
                lfasm_handle **out) {
@@ -1075,7 +1100,7 @@ static int gather(lfasm_handle *h, bool raw, int eliminate) {
   k_gather<R, L><<<grid, wpb * 32, sm, h->stream>>>(rows, h->long_rows, h->ea_ptr, h->ea,      \
                                                     h->off, h->I, h->Jc, h->Ae, h->nd, rs,     \
                                                     h->ess, h->sign, h->dof, eliminate, cap,   \
-                                                    h->vals)
+                                                    (long long)h->ne * h->nd, h->vals)
   if (raw) {
     LF_CUDA(cudaFuncSetAttribute(k_gather<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_optin));
     LF_GATHER(true, false, nb, h->n, smem);
@@ -1409,6 +1434,7 @@ int lfasm_batch_assemble(lfasm_batch *b, int eliminate) {
   LF_CUDA(cudaGraphLaunch(b->exec[slot], st));
   g_launches.fetch_add(b->kernels[slot], std::memory_order_relaxed);
   LF_CUDA(cudaStreamSynchronize(st));
+  if (int rb = bounds_status()) return rb;
   for (size_t i = 0; i < b->hs.size(); ++i) {
     lfasm_handle *h = b->hs[i];
     if (h->pml_variant != 1) continue;

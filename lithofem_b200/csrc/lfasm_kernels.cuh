@@ -22,6 +22,18 @@
 
 namespace lfasm_dev {
 
+// Bounds-checked debug build (-DLFASM_BOUNDS): index checks in the gather
+// record the code of the first failure in g_bounds_err and skip the access
+// (never trap); the host reads the word after each synchronising call.
+#ifdef LFASM_BOUNDS
+__device__ int g_bounds_err;
+#define LF_CHECK(cond, code) ((cond) ? true : (atomicCAS(&g_bounds_err, 0, (code)), false))
+#else
+#define LF_CHECK(cond, code) true
+#endif
+constexpr int BOUNDS_SLOT = 1;      // slot offset outside its CSR row
+constexpr int BOUNDS_ELEM_ROW = 2;  // row-list entry outside the element buffer
+
 struct dcplx {
   double re, im;
 };
@@ -1109,7 +1121,8 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
                                            const dcplx *__restrict__ Ae, int nd, int rs,
                                            const unsigned char *__restrict__ ess,
                                            const double *__restrict__ sign,
-                                           const int *__restrict__ dof, int eliminate) {
+                                           const int *__restrict__ dof, int eliminate,
+                                           long long n_erows) {
   for (int j = lane; j < nr; j += 32) acc[j] = mk(0.0, 0.0);
   __syncwarp();
   const bool row_ess = eliminate && ess[r];
@@ -1125,8 +1138,12 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
       dcplx v = mk(0.0, 0.0);
       int j = -1;
       if (sub < epi && pp < p1) {
-        v = Ae[(size_t)ea[pp] * rs + b];
-        j = off[(size_t)pp * nd + b];
+        const int id = ea[pp];
+        if (LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) {
+          v = Ae[(size_t)id * rs + b];
+          j = off[(size_t)pp * nd + b];
+          if (!LF_CHECK(j < nr, BOUNDS_SLOT)) j = -1;
+        }
       }
       for (int t = 0; t < epi; ++t) {
         if (sub == t && j >= 0) { acc[j].re += v.re; acc[j].im += v.im; }
@@ -1135,7 +1152,8 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
     }
   } else {
     for (int pp = ea_ptr[r]; pp < p1; ++pp) {
-      const int id = ea[pp];
+      const int id = ea[pp];  // the same in every lane
+      if (!LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) continue;
       const dcplx *src = Ae + (size_t)id * rs;
       const uint16_t *o = off + (size_t)pp * nd;
       double sa = 1.0;
@@ -1144,6 +1162,7 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
       for (int b = lane; b < nd; b += 32) {
         dcplx v = src[b];
         const int j = o[b];
+        if (!LF_CHECK(j < nr, BOUNDS_SLOT)) continue;
         if (RAW) {
           const double s = sa * sign[ebase + b];
           v.re *= s; v.im *= s;
@@ -1177,7 +1196,7 @@ __global__ void k_gather(int n, const int *__restrict__ long_rows, const int *__
                          const int *__restrict__ Jc, const dcplx *__restrict__ Ae, int nd, int rs,
                          const unsigned char *__restrict__ ess,
                          const double *__restrict__ sign, const int *__restrict__ dof,
-                         int eliminate, int maxrow, dcplx *__restrict__ vals) {
+                         int eliminate, int maxrow, long long n_erows, dcplx *__restrict__ vals) {
   extern __shared__ dcplx sacc[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int w = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1187,7 +1206,7 @@ __global__ void k_gather(int n, const int *__restrict__ long_rows, const int *__
   if (!LONG && nr > maxrow) return;
   dcplx *acc = LONG ? vals + rb : sacc + (size_t)wib * maxrow;
   gather_row<RAW>(acc, r, rb, nr, lane, ea_ptr, ea, off, Jc, Ae, nd, rs, ess, sign, dof,
-                  eliminate);
+                  eliminate, n_erows);
   if (!LONG)
     for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
 }

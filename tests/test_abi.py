@@ -99,3 +99,15 @@ def test_injected_failure(monkeypatch, capfd):
     assert rc == 6 and not h.value
     assert b"LITHOFEM_ASM_FORCE_FAIL" in _lib.lib().lfasm_last_error()
     assert "asm_gpu: forced failure injected (LITHOFEM_ASM_FORCE_FAIL)" in capfd.readouterr().out
+
+
+def test_bounds_checked_build_loads():
+    """The debug build with device index checks exports the same entry
+    points and reports itself; the production build reports 0."""
+    from pathlib import Path
+    dbg = Path(_lib.__file__).resolve().parent / "liblfasm_bounds.so"
+    L = ct.CDLL(str(dbg))
+    for name in _lib.exported_symbols():
+        assert hasattr(L, name), name
+    assert L.lfasm_bounds_checked() == 1
+    assert _lib.lib().lfasm_bounds_checked() == 0

@@ -1,0 +1,46 @@
+"""The bounds-checked debug build (liblfasm_bounds.so, device index checks
+in the gather) on parity cases: no check fires and the values match the
+oracle.  Runs in a child process because the library is loaded once per
+process (LFASM_LIBRARY selects the build)."""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+
+SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, %(root)r)
+from lithofem_b200 import _lib, configs
+from lithofem_b200.asm import AsmGpuGlobal
+from oracle import oracle
+assert _lib.lib().lfasm_bounds_checked() == 1
+cases = [configs.small_case("grating", 1, 6.0, seed=13, h=1.8),
+         configs.small_case("hole", 2, 6.0, seed=13, h=2.4),
+         configs.small_poly_case(3, 6.0, seed=5)]
+for c in cases:
+    g = AsmGpuGlobal(c.prob)
+    assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess)
+    I, J = oracle.csr(c.ad)
+    for elim in (False, True):
+        assert g.Assemble(elim), g.last_error
+        ref = oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, elim)
+        r = np.abs(g.DownloadValues() - ref).max() / np.abs(ref).max()
+        assert r < 1e-13, r
+print("bounds build ok")
+"""
+
+
+def test_bounds_checked_build_on_parity_cases():
+    env = dict(os.environ, LFASM_LIBRARY=str(ROOT / "lithofem_b200" / "liblfasm_bounds.so"))
+    out = subprocess.run([sys.executable, "-c", SCRIPT % {"root": str(ROOT)}], env=env,
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    assert "bounds build ok" in out.stdout
