@@ -16,6 +16,7 @@
 #include <map>
 #include <atomic>
 #include <mutex>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -955,6 +956,12 @@ int lfasm_download_local(lfasm_handle *h, double *host_out) {
 static int build_maps(lfasm_handle *h, const int *hI, const int *hJ, long long nnz_given) {
   const int n = h->n, nd = h->nd;
   const long long total = (long long)h->ne * nd;
+  // int32 CSR (the cuDSS contract) and int32 row-list positions: the
+  // candidate count ne * nd^2 bounds nnz and every position used here
+  if (total * nd > (long long)INT_MAX)
+    return fail(LFASM_ERR_UNSUPPORTED,
+                "%lld element couplings exceed the int32 CSR (ne * nd^2 must stay below 2^31)",
+                total * nd);
   int *cnt = nullptr, *fill = nullptr, *dmax = nullptr, *err = nullptr;
   int *tmpJ = nullptr;  // every row's unique columns at its candidate offset
   unsigned char *tmp = nullptr;
