@@ -668,6 +668,7 @@ def run_batch_e2e(a, cases, dev, torch) -> dict | None:
     total = sum(c.nnz for c in cases)
     outs = [torch.empty(2 * c.nnz, dtype=torch.float64, pin_memory=True) for c in cases]
     times = []
+    parts = []
     for it in range(1 + a.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -676,24 +677,31 @@ def run_batch_e2e(a, cases, dev, torch) -> dict | None:
             g = AsmGpuGlobal(c.prob)
             assert g.Init(ad, dev) and g.BuildGlobal(ad.ess)
             hs.append(g)
+        ta = time.perf_counter()
         b = AsmBatch(hs)
         assert b.Assemble(True)
+        tb = time.perf_counter()
         for g, o in zip(hs, outs):
             _, _, V, _, nz = g._csr()
             o.copy_(torch.as_tensor(DeviceVector(V, (2 * nz,), "<f8"), device="cuda"),
                     non_blocking=True)
         torch.cuda.synchronize()
+        tc = time.perf_counter()
         b.Release()
         for g in hs:
             g.Release()
         t1 = time.perf_counter()
         if it >= 1:
             times.append(t1 - t0)
+            parts.append([ta - t0, tb - ta, tc - tb, t1 - tc])
     t = float(np.median(times))
     return {"value": total / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(16 * total), "ms_per_step": 1e3 * t,
             "what": "per mesh lfasm_init (pinned host arrays) + lfasm_build_global, one "
                     "lfasm_batch_assemble (graph capture included), D2H of all CSR values",
+            "breakdown_ms": dict(zip(["init+build_global (16 handles)",
+                                      "batch create+capture+assemble", "d2h", "release"],
+                                     (np.median(np.array(parts), axis=0) * 1e3).tolist())),
             "timer": "host wall clock with device synchronize on both sides"}
 
 

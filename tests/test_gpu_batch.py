@@ -84,6 +84,39 @@ def test_batch_equals_per_handle_assembly():
     assert hs[0].Assemble(True)
 
 
+def test_handles_built_from_threads():
+    """lfasm_init / lfasm_build_global from several host threads at once
+    (the library's caches and memory pool are shared): every handle then
+    assembles exactly what it does when built alone."""
+    import concurrent.futures as cf
+    cases = [poly(1, 6.0, 3), poly(2, 6.0, 4), poly(3, 6.0, 5),
+             configs.small_case("hole", 2, 6.0, seed=13, h=2.4)]
+
+    def make(c):
+        g = AsmGpuGlobal(c.prob)
+        ok = g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess)
+        return g, ok
+
+    ref = []
+    for c in cases:
+        g, ok = make(c)
+        assert ok and g.Assemble(True)
+        ref.append(g.DownloadValues())
+        g.Release()
+    for _ in range(2):
+        with cf.ThreadPoolExecutor(max_workers=len(cases)) as ex:
+            built = list(ex.map(make, cases))
+        assert all(ok for _, ok in built)
+        hs = [g for g, _ in built]
+        b = AsmBatch(hs)
+        assert b.Assemble(True)
+        for g, r in zip(hs, ref):
+            np.testing.assert_array_equal(g.DownloadValues(), r)
+        b.Release()
+        for g in hs:
+            g.Release()
+
+
 def test_batch_argument_errors():
     with pytest.raises(RuntimeError, match="empty batch"):
         AsmBatch([])
