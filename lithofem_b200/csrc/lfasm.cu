@@ -1262,30 +1262,31 @@ int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3) {
   return LFASM_OK;
 }
 
+// the kernel variants of a handle that has none set: the per-process cached
+// decision for its kind of mesh, else the autotuner
+static int ensure_tuned(lfasm_handle *h) {
+  if (h->tuned) return LFASM_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(tune_key(h));
+    if (it != g_tune.end()) {
+      h->bulk_variant = it->second.variant;
+      for (int v = 0; v < 3; ++v) h->tune_ms[v] = it->second.ms[v];
+      if (!h->pml_forced) h->pml_variant = it->second.pml_variant;
+      h->pml_ms[0] = it->second.pml_ms[0];
+      h->pml_ms[1] = it->second.pml_ms[1];
+      h->tuned = 1;
+      return LFASM_OK;
+    }
+  }
+  return lfasm_autotune(h);
+}
+
 int lfasm_assemble(lfasm_handle *h, int eliminate) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   g_err.clear();
   if (!h->built) return fail(LFASM_ERR_STATE, "lfasm_build_global has not run");
-  if (!h->tuned) {
-    bool hit = false;
-    {
-      std::lock_guard<std::mutex> lk(g_tune_mu);
-      auto it = g_tune.find(tune_key(h));
-      if (it != g_tune.end()) {
-        hit = true;
-        h->bulk_variant = it->second.variant;
-        for (int v = 0; v < 3; ++v) h->tune_ms[v] = it->second.ms[v];
-        if (!h->pml_forced) h->pml_variant = it->second.pml_variant;
-        h->pml_ms[0] = it->second.pml_ms[0];
-        h->pml_ms[1] = it->second.pml_ms[1];
-        h->tuned = 1;
-      }
-    }
-    if (!hit) {
-      int rt = lfasm_autotune(h);
-      if (rt) return rt;
-    }
-  }
+  if (int rt = ensure_tuned(h)) return rt;
   const int mm = LFASM_MASS | (h->has_kpar ? (LFASM_CROSS0 | LFASM_CROSS1 | LFASM_KLK) : 0);
   int rc = launch_local(h, LFASM_CURLCURL, mm, 1, 1, eliminate ? 1 : 0);
   if (rc) return rc;
@@ -1333,10 +1334,7 @@ void batch_free(lfasm_batch *b) {
 int batch_capture(lfasm_batch *b, int eliminate) {
   const int slot = eliminate ? 1 : 0;
   for (lfasm_handle *h : b->hs)
-    if (!h->tuned) {
-      int rt = lfasm_autotune(h);
-      if (rt) return rt;
-    }
+    if (int rt = ensure_tuned(h)) return rt;
   LF_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
   int rc = LFASM_OK;
   cudaError_t ce = cudaEventRecord(b->fork, b->cs);
