@@ -176,10 +176,26 @@ void dfree(T *&p) {
 }
 
 struct DevRule {
-  int nq = 0;
+  int nq = 0, ldt = 0;
   double *ip = nullptr, *w = nullptr, *v = nullptr, *c = nullptr;
-  Rule view() const { Rule r; r.nq = nq; r.ip = ip; r.w = w; r.v = v; r.c = c; return r; }
+  double *vt = nullptr, *ct = nullptr;  // component-major, zero-padded columns
+  Rule view() const {
+    Rule r;
+    r.nq = nq; r.ip = ip; r.w = w; r.v = v; r.c = c; r.vt = vt; r.ct = ct; r.ldt = ldt;
+    return r;
+  }
 };
+
+// [q][k][d] (k < nd) -> [d][q][k] with ldt columns, zero past nd
+std::vector<double> component_major(const double *t, int nq, int nd, int ldt) {
+  std::vector<double> out((size_t)3 * nq * ldt, 0.0);
+  if (!t) return out;
+  for (int d = 0; d < 3; ++d)
+    for (int q = 0; q < nq; ++q)
+      for (int k = 0; k < nd; ++k)
+        out[((size_t)d * nq + q) * ldt + k] = t[((size_t)q * nd + k) * 3 + d];
+  return out;
+}
 
 }  // namespace
 
@@ -616,7 +632,12 @@ int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
     if ((e = upload(d.ip, r.ip, (size_t)r.nq * 3)) != cudaSuccess) return e;
     if ((e = upload(d.w, r.w, (size_t)r.nq)) != cudaSuccess) return e;
     if (r.vshape && (e = upload(d.v, r.vshape, (size_t)r.nq * nd * 3)) != cudaSuccess) return e;
-    return upload(d.c, r.curl, (size_t)r.nq * nd * 3);
+    if ((e = upload(d.c, r.curl, (size_t)r.nq * nd * 3)) != cudaSuccess) return e;
+    d.ldt = (nd + 7) & ~7;
+    const std::vector<double> vt = component_major(r.vshape, r.nq, nd, d.ldt);
+    const std::vector<double> ct = component_major(r.curl, r.nq, nd, d.ldt);
+    if ((e = upload(d.vt, vt.data(), vt.size())) != cudaSuccess) return e;
+    return upload(d.ct, ct.data(), ct.size());
   };
   LF_CUDA_H(up_rule(h->rcc, ad->rule_cc));
   LF_CUDA_H(up_rule(h->rm, ad->rule_mass));
@@ -1884,7 +1905,9 @@ void lfasm_destroy(lfasm_handle *h) {
   if (h->side) cudaStreamSynchronize(h->side);
   dfree(h->dof); dfree(h->sign); dfree(h->attr); dfree(h->J); dfree(h->Jinv); dfree(h->detJ);
   dfree(h->v0); dfree(h->fopack); dfree(h->signmask); dfree(h->essmask);
-  for (DevRule *r : {&h->rcc, &h->rm}) { dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); }
+  for (DevRule *r : {&h->rcc, &h->rm}) {
+    dfree(r->ip); dfree(r->w); dfree(r->v); dfree(r->c); dfree(r->vt); dfree(r->ct);
+  }
   dfree(h->eps_tab); dfree(h->elem_eps); dfree(h->bulk_list); dfree(h->pml_list);
   dfree(h->S); dfree(h->err); dfree(h->bexps); dfree(h->bcoef); dfree(h->bccoef); dfree(h->rec); dfree(h->S_mma); dfree(h->S_mmaf); dfree(h->rec_mma); dfree(h->Ae); dfree(h->slab_of); dfree(h->delta);
   dfree(h->src_list); dfree(h->src_slot); dfree(h->I); dfree(h->Jc); dfree(h->vals);

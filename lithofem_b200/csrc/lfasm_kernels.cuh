@@ -47,6 +47,10 @@ struct PmlParams {  // asm_gpu.inc:31-36
 struct Rule {
   int nq;
   const double *ip, *w, *v, *c;
+  // component-major copies, [d][q][k] with ldt (nd rounded up to 8, zero
+  // padded) columns: a column pair is one aligned 16-byte load
+  const double *vt, *ct;
+  int ldt;
 };
 
 constexpr int REC = 28;        // doubles per bulk-element coefficient record
@@ -718,21 +722,21 @@ __device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule
                                                unsigned sfo, const QCoef &C, double *Xs,
                                                double *Yr, double *Yi) {
   double v[2][3], c[2][3];
+  {
+    // reference shapes / curls of columns 2 pr, 2 pr + 1 (zero past nd)
+    double2 rv[3], rc[3];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int k = 2 * pr + h;
+    for (int r = 0; r < 3; ++r) {
+      const size_t o = ((size_t)r * R.nq + q) * R.ldt + 2 * pr;
+      rv[r] = need_v ? *reinterpret_cast<const double2 *>(R.vt + o) : make_double2(0.0, 0.0);
+      rc[r] = need_c ? *reinterpret_cast<const double2 *>(R.ct + o) : make_double2(0.0, 0.0);
+    }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { v[h][d] = 0.0; c[h][d] = 0.0; }
-    if (k < nd) {
-      const double *rv = R.v + ((size_t)q * nd + k) * 3;
-      const double *rc = R.c + ((size_t)q * nd + k) * 3;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (need_v)
-          v[h][d] = rv[0] * sJi[0 * 3 + d] + rv[1] * sJi[1 * 3 + d] + rv[2] * sJi[2 * 3 + d];
-        if (need_c)
-          c[h][d] = (rc[0] * sJ[d * 3 + 0] + rc[1] * sJ[d * 3 + 1] + rc[2] * sJ[d * 3 + 2]) * sidet;
-      }
+    for (int d = 0; d < 3; ++d) {
+      v[0][d] = rv[0].x * sJi[0 * 3 + d] + rv[1].x * sJi[1 * 3 + d] + rv[2].x * sJi[2 * 3 + d];
+      v[1][d] = rv[0].y * sJi[0 * 3 + d] + rv[1].y * sJi[1 * 3 + d] + rv[2].y * sJi[2 * 3 + d];
+      c[0][d] = (rc[0].x * sJ[d * 3 + 0] + rc[1].x * sJ[d * 3 + 1] + rc[2].x * sJ[d * 3 + 2]) * sidet;
+      c[1][d] = (rc[0].y * sJ[d * 3 + 0] + rc[1].y * sJ[d * 3 + 1] + rc[2].y * sJ[d * 3 + 2]) * sidet;
     }
   }
   if (te && p >= 2) {
