@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
@@ -458,17 +459,39 @@ void build_tinv(double out[24]) {
 // branch-free reduction (vectorised) and locates the index only in a block
 // that has one
 template <class F>
-size_t first_bad(size_t n, F bad) {
+size_t first_bad_range(size_t lo, size_t hi, F &bad) {
   constexpr size_t B = 8192;
-  for (size_t c = 0; c < n; c += B) {
-    const size_t e = std::min(n, c + B);
+  for (size_t c = lo; c < hi; c += B) {
+    const size_t e = std::min(hi, c + B);
     int any = 0;
     for (size_t i = c; i < e; ++i) any |= bad(i);
     if (any)
       for (size_t i = c; i < e; ++i)
         if (bad(i)) return i;
   }
-  return n;
+  return hi;
+}
+
+// large arrays are split over a few host threads; the answer is still the
+// lowest offending index
+template <class F>
+size_t first_bad(size_t n, F bad) {
+  constexpr size_t PAR_MIN = size_t(1) << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = n < PAR_MIN ? 1u : std::min(8u, hw);
+  if (nt == 1) return first_bad_range(0, n, bad);
+  std::vector<size_t> res(nt, n);
+  std::vector<std::thread> th;
+  const size_t step = (n + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const size_t lo = std::min(n, t * step), hi = std::min(n, lo + step);
+    th.emplace_back([&, t, lo, hi] {
+      const size_t r = first_bad_range(lo, hi, bad);
+      res[t] = r < hi ? r : n;
+    });
+  }
+  for (std::thread &x : th) x.join();
+  return *std::min_element(res.begin(), res.end());
 }
 
 // reference S tables depend only on p and the two rules: cached per process

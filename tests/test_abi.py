@@ -111,3 +111,31 @@ def test_bounds_checked_build_loads():
         assert hasattr(L, name), name
     assert L.lfasm_bounds_checked() == 1
     assert _lib.lib().lfasm_bounds_checked() == 0
+
+
+def test_validation_of_large_arrays_reports_the_lowest_index():
+    """Arrays above a million entries are scanned by several host threads;
+    the message still names the lowest offending entry."""
+    c = configs.small_case("slab", 1, 0.0)
+    ne = 400_000
+    nd = c.ad.nd
+    reps = -(-ne // c.ad.ne)
+    dof = np.tile(c.ad.dof.reshape(c.ad.ne, nd), (reps, 1))[:ne].reshape(-1).astype(np.int32)
+    attr = np.tile(c.ad.attr, reps)[:ne].astype(np.int32)
+    detJ = np.tile(c.ad.detJ, reps)[:ne].copy()
+    bad = dof.copy()
+    bad[[2_100_000, 1_900_000, 1_400_001]] = -1
+    m = _abi.marshal(c.ad, c.prob)
+    m.ad.ne = ne
+    keep = [bad, attr, detJ]
+    m.ad.dof = bad.ctypes.data_as(_abi.c_int_p)
+    m.ad.attr = attr.ctypes.data_as(_abi.c_int_p)
+    m.ad.detJ = detJ.ctypes.data_as(_abi.c_double_p)
+    h = ct.c_void_p()
+    rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
+    assert rc == 1 and _lib.lib().lfasm_last_error().startswith(b"dof[1400001] = -1")
+    detJ[[399_000, 250_001]] = 0.0
+    m.ad.dof = dof.ctypes.data_as(_abi.c_int_p)
+    rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
+    assert rc == 1 and _lib.lib().lfasm_last_error() == b"detJ[250001] not positive"
+    del keep
