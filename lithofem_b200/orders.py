@@ -83,3 +83,30 @@ def zeroth_order_efficiency(c00: np.ndarray, z: float, z_ref: float, kpar, k0: f
     qz_in = np.sqrt(complex(k0 ** 2 * eps_in - kpar[0] ** 2 - kpar[1] ** 2))
     inc_flux = 0.5 * (qz_in.real / k0) * lx * ly
     return direction * plane_wave_flux(c, kpar[0], kpar[1], qz, k0, direction, lx * ly) / inc_flux
+
+
+def incident_flux(k0: float, eps_in: complex, kx: float, ky: float, area: float) -> float:
+    """z-flux of a unit-amplitude incident plane wave through the cell
+    (outputs.py:235-238)."""
+    qz_in = np.sqrt(complex(k0 ** 2 * eps_in - kx ** 2 - ky ** 2))
+    return 0.5 * (qz_in.real / k0) * area
+
+
+def order_efficiencies(oset: OrderSet, z: float, z_ref: float, direction: int, area: float,
+                       inc_flux: float, bg00: np.ndarray | None = None
+                       ) -> dict[tuple[int, int], float]:
+    """Efficiency (flux / incident flux) of every order of a one-way region
+    (outputs.py:219-269).  direction +1: reflection side, up-going orders
+    sampled at height z; -1: transmission side, down-going.  Each scattered
+    coefficient is carried from z to the reference plane z_ref (the domain's
+    top or bottom); bg00 is the analytic (0,0) background at z_ref (the
+    reflected wave above, the transmitted wave below) and adds to the (0,0)
+    order there."""
+    out: dict[tuple[int, int], float] = {}
+    for i in range(len(oset.ms)):
+        c = oset.coeffs[i] * np.exp(-1j * direction * oset.qz[i] * (z - z_ref))
+        if oset.ms[i] == 0 and oset.ns[i] == 0 and bg00 is not None:
+            c = c + bg00
+        out[(int(oset.ms[i]), int(oset.ns[i]))] = direction * plane_wave_flux(
+            c, oset.kx[i], oset.ky[i], oset.qz[i], oset.k0, direction, area) / inc_flux
+    return out
