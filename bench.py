@@ -52,9 +52,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pml-variant", type=int, default=-1,
-                    help="force the p = 3 PML kernel (0 k_pml_mma, 1 k_pml_ws); default: autotune")
+                    help="force the PML kernel (0 k_pml_mma, 1 k_pml_ws at p = 3, 2 k_pml_sym); "
+                         "default: autotune")
     ap.add_argument("--bulk-variant", type=int, default=-1,
-                    help="force the bulk-element kernel (0 SIMT, 1 DMMA); default: autotune")
+                    help="force the bulk-element kernel (0 SIMT, 1/2 DMMA with 4/2 tiles a warp, "
+                         "3/4 the same without block barriers); default: autotune")
     return ap.parse_args()
 
 
@@ -119,6 +121,28 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": float(max(smax)) if smax else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
+
+
+PML_KERNELS = ["k_pml_mma", "k_pml_ws", "k_pml_sym"]
+BULK_KERNELS = ["k_bulk (SIMT)", "k_bulk_mma<4 tiles/warp> (DMMA)", "k_bulk_mma<2 tiles/warp> (DMMA)",
+                "k_bulk_mma_nb<4 tiles/warp> (DMMA, no block barriers)",
+                "k_bulk_mma_nb<2 tiles/warp> (DMMA, no block barriers)"]
+
+
+def pml_flops(n_pml: int, nd: int, nq_cc: int, nq_mass: int, cross: bool, variant: int) -> float:
+    """Algorithmic FP64 flops of the PML element kernel (real x complex
+    multiply-adds, 4 flops per staged row and matrix entry).  k_pml_mma and
+    k_pml_ws form every entry of X^T (W X): 3 rows per curl point, 3 (6 with
+    the cross terms) per mass point.  k_pml_sym forms the symmetric part on
+    and above the diagonal (3 rows per point of both rules) and every entry
+    of the cross part (3 rows per mass point)."""
+    if variant == 2:
+        f = 4.0 * 3 * (nq_cc + nq_mass) * nd * (nd + 1) / 2
+        if cross:
+            f += 4.0 * 3 * nq_mass * nd * nd
+    else:
+        f = 4.0 * (3 * nq_cc + (6 if cross else 3) * nq_mass) * nd * nd
+    return n_pml * f
 
 
 def fp64_peak_tflops(torch) -> float:
@@ -391,8 +415,7 @@ def run_ours(a, rank, world, local, dist, torch):
                   + case.nnz * 16,
     }
     rm, rc = ad.rule_mass, ad.rule_cc
-    rows = 3 * rc.nq + (6 if prob.has_kpar else 3) * rm.nq
-    pml_flops = npml * 4.0 * rows * nd * nd
+    flops_pml = pml_flops(npml, nd, rc.nq, rm.nq, prob.has_kpar, pml_tuning[0])
     fp64 = fp64_peak_tflops(torch)
     stage_names = ["prep+bulk", "pml", "gather"]
     kern = {}
@@ -400,11 +423,11 @@ def run_ours(a, rank, world, local, dist, torch):
         kern[nm] = {"ms": float(t), "share": float(t / stages.sum())}
     kern["prep+bulk"]["GB/s"] = alg["bulk"] / (stages[0] * 1e-3) / 1e9
     kern["gather"]["GB/s"] = alg["gather"] / (stages[2] * 1e-3) / 1e9
-    kern["pml"]["TFLOP/s"] = pml_flops / (stages[1] * 1e-3) / 1e12 if stages[1] > 0 else 0.0
+    kern["pml"]["TFLOP/s"] = flops_pml / (stages[1] * 1e-3) / 1e12 if stages[1] > 0 else 0.0
     top = int(np.argmax(stages))
     if top == 1:
         ach = kern["pml"]["TFLOP/s"]
-        roof = {"kernel": "k_pml_ws" if pml_tuning[0] == 1 else "k_pml_mma",
+        roof = {"kernel": PML_KERNELS[pml_tuning[0]],
                 "what": "PML elements, FP64 quadrature contraction on DMMA",
                 "bound": "tensor",
                 "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
@@ -412,7 +435,7 @@ def run_ours(a, rank, world, local, dist, torch):
     else:
         nm = stage_names[top]
         ach = kern[nm]["GB/s"]
-        roof = {"kernel": {"prep+bulk": "k_bulk_mma" if tuning[0] else "k_bulk",
+        roof = {"kernel": {"prep+bulk": BULK_KERNELS[tuning[0]].split("<")[0].split(" ")[0],
                            "gather": "k_gather"}[nm], "bound": "hbm",
                 "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
@@ -443,10 +466,9 @@ def run_ours(a, rank, world, local, dist, torch):
             "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
-            "tuning": {"bulk_variant": ["k_bulk (SIMT)", "k_bulk_mma<4 tiles/warp> (DMMA)",
-                                        "k_bulk_mma<2 tiles/warp> (DMMA)"][tuning[0]],
+            "tuning": {"bulk_variant": BULK_KERNELS[tuning[0]],
                        "bulk_ms": tuning[1],
-                       "pml_variant": ["k_pml_mma", "k_pml_ws (warp-specialised)"][pml_tuning[0]],
+                       "pml_variant": PML_KERNELS[pml_tuning[0]],
                        "pml_ms": pml_tuning[1]}}
     print(json.dumps(line), flush=True)
     g.Release()
@@ -543,8 +565,11 @@ def run_batch(a, rank, world, local, dist, torch):
     stages = np.zeros(3)
     serial_ms = 0.0
     per_mesh = []
+    pml_var, bulk_var = [], []
     for g in hs:
         assert g.Assemble(True)          # tunes the handle
+        pml_var.append(g.PmlTuning()[0])
+        bulk_var.append(g.Tuning()[0])
         assert g.SetProfile(True)
         assert g.Assemble(True)
         st = np.array(g.StageTimes())
@@ -592,13 +617,15 @@ def run_batch(a, rank, world, local, dist, torch):
              + c.nnz * 16 for c in cases)
     kern["gather"]["GB/s"] = gb / (stages[2] * 1e-3) / 1e9
     flops = 0.0
-    for c in cases:
-        rows = 3 * c.ad.rule_cc.nq + (6 if c.prob.has_kpar else 3) * c.ad.rule_mass.nq
-        flops += float(np.sum(_pml_mask(c))) * 4.0 * rows * c.ad.nd ** 2
+    for c, v in zip(cases, pml_var):
+        flops += pml_flops(int(np.sum(_pml_mask(c))), c.ad.nd, c.ad.rule_cc.nq,
+                           c.ad.rule_mass.nq, c.prob.has_kpar, v)
     kern["pml"]["TFLOP/s"] = flops / (stages[1] * 1e-3) / 1e12 if stages[1] > 0 else 0.0
+    kern["pml"]["variants"] = [PML_KERNELS[v] for v in pml_var]
     top = int(np.argmax(stages))
     if top == 1:
-        roof = {"kernel": "k_pml_mma", "bound": "tensor", "achieved": kern["pml"]["TFLOP/s"],
+        roof = {"kernel": "/".join(sorted({PML_KERNELS[v] for v in pml_var})), "bound": "tensor",
+                "achieved": kern["pml"]["TFLOP/s"],
                 "peak": fp64, "unit": "TFLOP/s", "frac": kern["pml"]["TFLOP/s"] / fp64,
                 "peak_source": "measured in-run: cuBLAS DGEMM 8192^3", "traffic": None}
     else:
@@ -606,7 +633,8 @@ def run_batch(a, rank, world, local, dist, torch):
         if nm == "prep+bulk":
             bb = sum(float(np.sum(~_pml_mask(c))) * (c.ad.nd ** 2 * 16 + 256) for c in cases)
             kern[nm]["GB/s"] = bb / (stages[0] * 1e-3) / 1e9
-        roof = {"kernel": {"gather": "k_gather", "prep+bulk": "k_bulk_mma"}[nm], "bound": "hbm",
+        bulk_names = "/".join(sorted({BULK_KERNELS[v].split("<")[0].split(" ")[0] for v in bulk_var}))
+        roof = {"kernel": {"gather": "k_gather", "prep+bulk": bulk_names}[nm], "bound": "hbm",
                 "achieved": kern[nm]["GB/s"], "peak": hbm, "unit": "GB/s",
                 "frac": kern[nm]["GB/s"] / hbm,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}

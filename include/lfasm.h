@@ -232,22 +232,27 @@ int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_
 
 /* Autotuner: times the bulk-element kernel variants on this mesh -- 0: the
  * SIMT k_bulk, 1 and 2: the FP64 tensor-core k_bulk_mma with 4 or 2 tiles
- * per warp -- and keeps the fastest.  The first lfasm_assemble of a handle
+ * per warp, 3 and 4: the same without block barriers (k_bulk_mma_nb) -- and
+ * keeps the fastest.  The first lfasm_assemble of a handle
  * whose variant was not set takes the decision from a per-process cache
  * keyed by device, order p, k-parallel terms and the power-of-two class of
  * the bulk element count, and runs the autotuner only on a miss; an explicit
  * lfasm_autotune always times and refreshes the cache.  lfasm_get_tuning
- * reports the choice and the three timings (ms). */
+ * reports the choice and one timing per variant (ms, LFASM_BULK_VARIANTS
+ * floats). */
+#define LFASM_BULK_VARIANTS 5
 int lfasm_autotune(lfasm_handle *h);
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant);
-int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3);
+int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms);
 
-/* The PML-element kernel at p = 3: 0 k_pml_mma, 1 k_pml_ws (warp-specialised
- * producer/consumer pipeline).  The autotuner times both on the mesh (the
- * cached decision carries it); lfasm_set_pml_variant fixes it (1 only at
- * p = 3).  lfasm_get_pml_tuning reports the choice and both timings (ms). */
+/* The PML-element kernel: 0 k_pml_mma, 1 k_pml_ws (warp-specialised
+ * producer/consumer pipeline, p = 3 only), 2 k_pml_sym (the element matrix
+ * split into its symmetric part, upper tiles only, and the cross part).  The
+ * autotuner times the variants on the mesh (the cached decision carries
+ * it); lfasm_set_pml_variant fixes one.  lfasm_get_pml_tuning reports the
+ * choice and three timings in ms (0 for a variant not timed). */
 int lfasm_set_pml_variant(lfasm_handle *h, int variant);
-int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms2);
+int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms3);
 
 /* Field sampling and the orders' adjoint seed (the reference samples planes
  * with MFEM FindPoints/GetVectorValue, solver/lithofem_solve.cpp:951-1004,

@@ -17,7 +17,8 @@ import ctypes as ct
 import numpy as np
 
 from . import _lib
-from ._abi import CROSS0, CROSS1, CURLCURL, KLK, MASS, c_double_p, c_int_p, marshal, marshal_parts
+from ._abi import (BULK_VARIANTS, CROSS0, CROSS1, CURLCURL, KLK, MASS, c_double_p, c_int_p, marshal,
+                   marshal_parts)
 from .problem import Problem
 from .space import AsmData
 
@@ -104,7 +105,7 @@ class AsmGpu:
 
     def Tuning(self) -> tuple[int, list[float]]:
         v = ct.c_int()
-        ms = (ct.c_float * 3)()
+        ms = (ct.c_float * BULK_VARIANTS)()
         _lib.check(_lib.lib().lfasm_get_tuning(self._h, ct.byref(v), ms))
         return v.value, [float(x) for x in ms]
 
@@ -113,7 +114,7 @@ class AsmGpu:
 
     def PmlTuning(self) -> tuple[int, list[float]]:
         v = ct.c_int()
-        ms = (ct.c_float * 2)()
+        ms = (ct.c_float * 3)()
         _lib.check(_lib.lib().lfasm_get_pml_tuning(self._h, ct.byref(v), ms))
         return v.value, [float(x) for x in ms]
 

@@ -226,14 +226,17 @@ struct lfasm_handle {
   // tensor-core bulk variant and the autotuned choice
   double *S_mma = nullptr, *rec_mma = nullptr;
   double *S_mmaf = nullptr;  // B operand of the fused Bloch layout
-  int bulk_variant = 0;      // 0: k_bulk (SIMT), 1/2: k_bulk_mma (DMMA, 4/2 tiles per warp)
+  // 0: k_bulk (SIMT), 1/2: k_bulk_mma (DMMA, 4/2 tiles per warp),
+  // 3/4: k_bulk_mma_nb (the same without block barriers, 4/2 tiles per warp)
+  int bulk_variant = 0;
   int tuned = 0;             // autotune done
   int forced = 0;            // variant fixed by lfasm_set_bulk_variant
-  float tune_ms[3] = {0.f, 0.f, 0.f};
-  // PML kernel at p = 3: 0 k_pml_mma, 1 k_pml_ws (warp-specialised)
+  float tune_ms[LFASM_BULK_VARIANTS] = {};
+  // PML kernel: 0 k_pml_mma, 1 k_pml_ws (warp-specialised, p = 3 only),
+  // 2 k_pml_sym (symmetric split)
   int pml_variant = 0;
   int pml_forced = 0;
-  float pml_ms[2] = {0.f, 0.f};
+  float pml_ms[3] = {0.f, 0.f, 0.f};
   int *err = nullptr;  // device error word of the bounded-wait kernels
   // element basis for sampling away from the quadrature points
   int nmono = 0;
@@ -836,7 +839,7 @@ int lfasm_path_counts(lfasm_handle *h, int *n_bulk, int *n_pml) {
 template <int NDP8>
 static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int mask_mass, int te,
                       int eliminate, int rs, cudaStream_t st) {
-  const size_t smem = PmlShape<NDP8>::smem(PmlShape<NDP8>::QC, h->rcc.nq + h->rm.nq);
+  size_t smem = PmlShape<NDP8>::smem(PmlShape<NDP8>::QC, h->rcc.nq + h->rm.nq);
   const int threads = NDP8 * 4;
   auto go = [&](auto kern) -> int {
     LF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -864,6 +867,12 @@ static int launch_pml(lfasm_handle *h, bool cross, int mode, int mask_cc, int ma
     };
     if (cross) return mode ? ws(k_pml_ws<true, 1>) : ws(k_pml_ws<true, 0>);
     return mode ? ws(k_pml_ws<false, 1>) : ws(k_pml_ws<false, 0>);
+  }
+  if (h->pml_variant == 2) {
+    // mask_cc never carries the cross bits, so cross = cross terms in mask_mass
+    smem = PmlSymShape<NDP8>::smem(h->rcc.nq + h->rm.nq, cross);
+    if (cross) return mode ? go(k_pml_sym<NDP8, true, 1>) : go(k_pml_sym<NDP8, true, 0>);
+    return mode ? go(k_pml_sym<NDP8, false, 1>) : go(k_pml_sym<NDP8, false, 0>);
   }
   if (cross) return mode ? go(k_pml_mma<NDP8, true, 1>) : go(k_pml_mma<NDP8, true, 0>);
   return mode ? go(k_pml_mma<NDP8, false, 1>) : go(k_pml_mma<NDP8, false, 0>);
@@ -922,7 +931,8 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
                                                              fused ? 1 : 0, h->rec_mma);
     LF_LAUNCHED();
     const int ntiles = bulk_tiles(h->ndp);
-    const int TT = h->bulk_variant == 1 ? 4 : 2;  // tiles per warp
+    const int TT = (h->bulk_variant == 1 || h->bulk_variant == 3) ? 4 : 2;  // tiles per warp
+    const bool nobar = h->bulk_variant >= 3;
     const int ytiles = (ntiles + BULK_WARPS * TT - 1) / (BULK_WARPS * TT);
     // k_bulk_mma writes 16-byte-aligned double4 pairs: needs rs even (the
     // fused layout); the dense ComputeLocal layout uses the SIMT kernel
@@ -931,7 +941,8 @@ static int launch_local(lfasm_handle *h, int mask_cc, int mask_mass, int te, int
     const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
     dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
 #define LF_BULKM(C, M, T, F)                                                      \
-  k_bulk_mma<C, M, T, F><<<grid, BULK_WARPS * 32, 0, h->stream>>>(                \
+  (nobar ? k_bulk_mma_nb<C, M, T, F> : k_bulk_mma<C, M, T, F>)                    \
+      <<<grid, BULK_WARPS * 32, 0, h->stream>>>(                                  \
       nb, h->bulk_list, h->rec_mma, F ? h->S_mmaf : h->S_mma, ntiles, h->nd, h->ndp, \
       h->p, bchunk, te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
 #define LF_BULKM_T(T, F)                                                          \
@@ -1185,9 +1196,9 @@ int lfasm_scatter_eliminate(lfasm_handle *h, int eliminate) {
 namespace {
 struct TuneEntry {
   int variant;
-  float ms[3];
+  float ms[LFASM_BULK_VARIANTS];
   int pml_variant;
-  float pml_ms[2];
+  float pml_ms[3];
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 4>, TuneEntry> g_tune;
@@ -1214,7 +1225,7 @@ int lfasm_autotune(lfasm_handle *h) {
   const int keep_n_pml = h->n_pml;
   h->n_pml = 0;  // time the bulk path alone
   int rc = LFASM_OK;
-  for (int v = 0; v < 3 && !rc; ++v) {
+  for (int v = 0; v < LFASM_BULK_VARIANTS && !rc; ++v) {
     h->bulk_variant = v;
     for (int rep = 0; rep < 2 && !rc; ++rep) {
       LF_CUDA(cudaEventRecord(a, h->stream));
@@ -1228,14 +1239,16 @@ int lfasm_autotune(lfasm_handle *h) {
   }
   h->n_pml = keep_n_pml;
   int best = 0;
-  for (int v = 1; v < 3; ++v)
+  for (int v = 1; v < LFASM_BULK_VARIANTS; ++v)
     if (h->tune_ms[v] < h->tune_ms[best]) best = v;
   h->bulk_variant = best;
-  if (!rc && h->p == 3 && h->n_pml > 0 && !h->pml_forced) {
-    // PML kernels at p = 3, the PML path alone
+  if (!rc && h->n_pml > 0 && !h->pml_forced) {
+    // PML kernels (the warp-specialised one at p = 3 only), the PML path alone
     const int keep_n_bulk = h->n_bulk;
     h->n_bulk = 0;
-    for (int v = 0; v < 2 && !rc; ++v) {
+    for (int v = 0; v < 3 && !rc; ++v) {
+      h->pml_ms[v] = 0.f;
+      if (v == 1 && h->p != 3) continue;
       h->pml_variant = v;
       for (int rep = 0; rep < 2 && !rc; ++rep) {
         LF_CUDA(cudaEventRecord(a, h->stream));
@@ -1252,7 +1265,12 @@ int lfasm_autotune(lfasm_handle *h) {
       int e = 0;
       LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
       // a variant whose waits ran out is never chosen
-      h->pml_variant = (e == 0 && h->pml_ms[1] < h->pml_ms[0]) ? 1 : 0;
+      int bestp = 0;
+      for (int v = 1; v < 3; ++v) {
+        if (h->pml_ms[v] <= 0.f || (v == 1 && e)) continue;
+        if (h->pml_ms[v] < h->pml_ms[bestp]) bestp = v;
+      }
+      h->pml_variant = bestp;
       if (e) LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
     }
   }
@@ -1265,17 +1283,17 @@ int lfasm_autotune(lfasm_handle *h) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     TuneEntry &t = g_tune[tune_key(h)];
     t.variant = best;
-    for (int v = 0; v < 3; ++v) t.ms[v] = h->tune_ms[v];
+    for (int v = 0; v < LFASM_BULK_VARIANTS; ++v) t.ms[v] = h->tune_ms[v];
     t.pml_variant = h->pml_variant;
-    t.pml_ms[0] = h->pml_ms[0];
-    t.pml_ms[1] = h->pml_ms[1];
+    for (int v = 0; v < 3; ++v) t.pml_ms[v] = h->pml_ms[v];
   }
   return sync_if(h);
 }
 
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
-  if (variant < 0 || variant > 2) return fail(LFASM_ERR_ARG, "bulk variant must be 0, 1 or 2");
+  if (variant < 0 || variant >= LFASM_BULK_VARIANTS)
+    return fail(LFASM_ERR_ARG, "bulk variant must be 0 .. %d", LFASM_BULK_VARIANTS - 1);
   h->bulk_variant = variant;
   h->forced = 1;
   h->tuned = 1;
@@ -1284,7 +1302,7 @@ int lfasm_set_bulk_variant(lfasm_handle *h, int variant) {
 
 int lfasm_set_pml_variant(lfasm_handle *h, int variant) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
-  if (variant < 0 || variant > 1) return fail(LFASM_ERR_ARG, "PML variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return fail(LFASM_ERR_ARG, "PML variant must be 0, 1 or 2");
   if (variant == 1 && h->p != 3)
     return fail(LFASM_ERR_UNSUPPORTED, "the warp-specialised PML kernel is for p = 3");
   h->pml_variant = variant;
@@ -1292,17 +1310,17 @@ int lfasm_set_pml_variant(lfasm_handle *h, int variant) {
   return LFASM_OK;
 }
 
-int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms2) {
+int lfasm_get_pml_tuning(lfasm_handle *h, int *pml_variant, float *ms3) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   if (pml_variant) *pml_variant = h->pml_variant;
-  if (ms2) for (int i = 0; i < 2; ++i) ms2[i] = h->pml_ms[i];
+  if (ms3) for (int i = 0; i < 3; ++i) ms3[i] = h->pml_ms[i];
   return LFASM_OK;
 }
 
-int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms3) {
+int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms) {
   if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
   if (bulk_variant) *bulk_variant = h->bulk_variant;
-  if (ms3) for (int i = 0; i < 3; ++i) ms3[i] = h->tune_ms[i];
+  if (ms) for (int i = 0; i < LFASM_BULK_VARIANTS; ++i) ms[i] = h->tune_ms[i];
   return LFASM_OK;
 }
 
@@ -1315,10 +1333,9 @@ static int ensure_tuned(lfasm_handle *h) {
     auto it = g_tune.find(tune_key(h));
     if (it != g_tune.end()) {
       h->bulk_variant = it->second.variant;
-      for (int v = 0; v < 3; ++v) h->tune_ms[v] = it->second.ms[v];
+      for (int v = 0; v < LFASM_BULK_VARIANTS; ++v) h->tune_ms[v] = it->second.ms[v];
       if (!h->pml_forced) h->pml_variant = it->second.pml_variant;
-      h->pml_ms[0] = it->second.pml_ms[0];
-      h->pml_ms[1] = it->second.pml_ms[1];
+      for (int v = 0; v < 3; ++v) h->pml_ms[v] = it->second.pml_ms[v];
       h->tuned = 1;
       return LFASM_OK;
     }

@@ -461,6 +461,73 @@ __global__ void k_prep_bulk_mma(int nb, const int *__restrict__ list,
     }
 }
 
+// One row-pair block of a bulk DMMA tile for 8 elements: the DMMA
+// contraction (every lane, the instruction is warp-wide), then for this
+// lane's element (ok) the dual face transform, signs and essential zeroing
+// and the store of c[a][i] = entry (row + a, col + i).
+template <bool CROSS, int MODE, int KS, bool FUSED>
+__device__ __forceinline__ void bulk_rowpair(const double (&bfj)[2][KS], const double (&ar)[3],
+                                             const double (&ai)[KS], bool ok, unsigned fp,
+                                             unsigned long long sm, unsigned long long em,
+                                             int row, int col, int fr, int fc, const double *sT,
+                                             int nd, int rs, dcplx *base) {
+  double cr[2][2], ci[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    cr[a][0] = cr[a][1] = ci[a][0] = ci[a][1] = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) dmma(cr[a][0], cr[a][1], ar[ks], bfj[a][ks]);
+    if (FUSED) {
+#pragma unroll
+      for (int ks = 3; ks < (CROSS ? 7 : 5); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bfj[a][ks]);
+    } else {
+#pragma unroll
+      for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bfj[a][ks]);
+    }
+  }
+  if (!ok) return;
+  if (fc >= 0) {  // columns: A <- A M
+    const double *T = sT + 4 * ((fp >> (8 * fc)) & 0xffu);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      const double n0 = T[0] * cr[a][0] + T[1] * cr[a][1], n1 = T[2] * cr[a][0] + T[3] * cr[a][1];
+      const double m0 = T[0] * ci[a][0] + T[1] * ci[a][1], m1 = T[2] * ci[a][0] + T[3] * ci[a][1];
+      cr[a][0] = n0; cr[a][1] = n1; ci[a][0] = m0; ci[a][1] = m1;
+    }
+  }
+  if (fr >= 0) {  // rows: A <- M^T A
+    const double *T = sT + 4 * ((fp >> (8 * fr)) & 0xffu);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const double n0 = T[0] * cr[0][i] + T[1] * cr[1][i], n1 = T[2] * cr[0][i] + T[3] * cr[1][i];
+      const double m0 = T[0] * ci[0][i] + T[1] * ci[1][i], m1 = T[2] * ci[0][i] + T[3] * ci[1][i];
+      cr[0][i] = n0; cr[1][i] = n1; ci[0][i] = m0; ci[1][i] = m1;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int r = row + a;
+    if (r >= nd) continue;
+    if (MODE == 1) {
+      const unsigned long long rbit = (sm >> r) & 1ull, cbits = sm >> col;
+      const double s0 = ((rbit ^ cbits) & 1ull) ? -1.0 : 1.0;
+      const double s1 = ((rbit ^ (cbits >> 1)) & 1ull) ? -1.0 : 1.0;
+      cr[a][0] *= s0; ci[a][0] *= s0; cr[a][1] *= s1; ci[a][1] *= s1;
+      const unsigned long long eb = em >> col;
+      const bool er = (em >> r) & 1ull;
+      if (er || (eb & 1ull)) { cr[a][0] = 0.0; ci[a][0] = 0.0; }
+      if (er || (eb & 2ull)) { cr[a][1] = 0.0; ci[a][1] = 0.0; }
+    }
+    dcplx *dst = base + (size_t)r * rs + col;
+    if (col + 1 < nd && (reinterpret_cast<uintptr_t>(dst) & 31u) == 0) {
+      reinterpret_cast<double4 *>(dst)[0] = make_double4(cr[a][0], ci[a][0], cr[a][1], ci[a][1]);
+    } else {
+      dst[0] = mk(cr[a][0], ci[a][0]);
+      if (col + 1 < nd) dst[1] = mk(cr[a][1], ci[a][1]);
+    }
+  }
+}
+
 // Tiles are 8 consecutive columns of one row: tile t = 2 (I * ncb + cb) + a
 // covers entry (2I + a, 8 cb + c), c = 0..7, so a warp's C fragment for one
 // element is one full 128-byte line of the (row-padded) element matrix.  A
@@ -562,65 +629,91 @@ k_bulk_mma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
     const unsigned long long sm = ssm[g], em = sem[g];
     dcplx *base = e >= 0 ? Ae + (size_t)e * nd * rs : Ae;
 #pragma unroll
-    for (int j = 0; j < PB; ++j) {
-      // c[a][i]: row 2I + a, column col + i
-      double cr[2][2], ci[2][2];
+    for (int j = 0; j < PB; ++j)
+      bulk_rowpair<CROSS, MODE, KS, FUSED>(bf[j], ar, ai, okv[j] && e >= 0, fp, sm, em, rowv[j],
+                                           colv[j], frv[j], fcv[j], sT, nd, rs, base);
+  }
+}
+
+// k_bulk_mma without block barriers: each lane reads the record terms and
+// the metadata of its own element (row g of the batch of 8) straight from
+// global memory -- the records are L2 resident and the block's warps share
+// them through L1 -- one batch ahead in registers, so the warps of a block
+// run independently.  Same tiles, operands and epilogue as k_bulk_mma.
+template <bool CROSS, int MODE, int TT, bool FUSED>
+__global__ void __launch_bounds__(BULK_WARPS * 32)
+k_bulk_mma_nb(int nb, const int *__restrict__ list, const double *__restrict__ rec,
+              const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk,
+              int te, int eliminate, int rs, const unsigned *__restrict__ fopack,
+              const unsigned long long *__restrict__ signmask,
+              const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
+  __shared__ double sT[24];
+  constexpr int PB = TT / 2;
+  constexpr int KS = FUSED ? 7 : BK / 4;
+  constexpr int RECW = FUSED ? BK : BREC;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int ncb = (ndp + 7) / 8;
+  const int npb = (ndp / 2) * ncb;
+  if (tid < 24) sT[tid] = c_tinv[tid];
+  double bf[PB][2][KS];
+  int rowv[PB], colv[PB], frv[PB], fcv[PB], okv[PB];
+  const int pb0 = (blockIdx.y * BULK_WARPS + w) * PB;
 #pragma unroll
-      for (int a = 0; a < 2; ++a) {
-        cr[a][0] = cr[a][1] = ci[a][0] = ci[a][1] = 0.0;
+  for (int j = 0; j < PB; ++j) {
+    const int pb = pb0 + j;
+    const bool ok = pb < npb;
 #pragma unroll
-        for (int ks = 0; ks < 3; ++ks) dmma(cr[a][0], cr[a][1], ar[ks], bf[j][a][ks]);
-        if (FUSED) {
+    for (int a = 0; a < 2; ++a) {
+      const int tile = 2 * pb + a;
 #pragma unroll
-          for (int ks = 3; ks < (CROSS ? 7 : 5); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
-        } else {
-#pragma unroll
-          for (int ks = 1; ks < (CROSS ? KS : 3); ++ks) dmma(ci[a][0], ci[a][1], ai[ks], bf[j][a][ks]);
-        }
-      }
-      if (!okv[j] || e < 0) continue;
-      if (fcv[j] >= 0) {  // columns: A <- A M
-        const double *T = sT + 4 * ((fp >> (8 * fcv[j])) & 0xffu);
-#pragma unroll
-        for (int a = 0; a < 2; ++a) {
-          const double n0 = T[0] * cr[a][0] + T[1] * cr[a][1], n1 = T[2] * cr[a][0] + T[3] * cr[a][1];
-          const double m0 = T[0] * ci[a][0] + T[1] * ci[a][1], m1 = T[2] * ci[a][0] + T[3] * ci[a][1];
-          cr[a][0] = n0; cr[a][1] = n1; ci[a][0] = m0; ci[a][1] = m1;
-        }
-      }
-      if (frv[j] >= 0) {  // rows: A <- M^T A
-        const double *T = sT + 4 * ((fp >> (8 * frv[j])) & 0xffu);
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const double n0 = T[0] * cr[0][i] + T[1] * cr[1][i], n1 = T[2] * cr[0][i] + T[3] * cr[1][i];
-          const double m0 = T[0] * ci[0][i] + T[1] * ci[1][i], m1 = T[2] * ci[0][i] + T[3] * ci[1][i];
-          cr[0][i] = n0; cr[1][i] = n1; ci[0][i] = m0; ci[1][i] = m1;
-        }
-      }
-      const int row = rowv[j], col = colv[j];
-#pragma unroll
-      for (int a = 0; a < 2; ++a) {
-        const int r = row + a;
-        if (r >= nd) continue;
-        if (MODE == 1) {
-          const unsigned long long rbit = (sm >> r) & 1ull, cbits = sm >> col;
-          const double s0 = ((rbit ^ cbits) & 1ull) ? -1.0 : 1.0;
-          const double s1 = ((rbit ^ (cbits >> 1)) & 1ull) ? -1.0 : 1.0;
-          cr[a][0] *= s0; ci[a][0] *= s0; cr[a][1] *= s1; ci[a][1] *= s1;
-          const unsigned long long eb = em >> col;
-          const bool er = (em >> r) & 1ull;
-          if (er || (eb & 1ull)) { cr[a][0] = 0.0; ci[a][0] = 0.0; }
-          if (er || (eb & 2ull)) { cr[a][1] = 0.0; ci[a][1] = 0.0; }
-        }
-        dcplx *dst = base + (size_t)r * rs + col;
-        if (col + 1 < nd && (reinterpret_cast<uintptr_t>(dst) & 31u) == 0) {
-          reinterpret_cast<double4 *>(dst)[0] = make_double4(cr[a][0], ci[a][0], cr[a][1], ci[a][1]);
-        } else {
-          dst[0] = mk(cr[a][0], ci[a][0]);
-          if (col + 1 < nd) dst[1] = mk(cr[a][1], ci[a][1]);
-        }
-      }
+      for (int ks = 0; ks < KS; ++ks)
+        bf[j][a][ks] = ok ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
     }
+    const int I = ok ? pb / ncb : 0, cb = ok ? pb - I * ncb : 0;
+    rowv[j] = 2 * I;
+    colv[j] = 8 * cb + 2 * t4;
+    okv[j] = ok && rowv[j] < nd && colv[j] < nd;
+    frv[j] = (te && p >= 2) ? face_of(2 * I, p) : -1;
+    fcv[j] = (te && p >= 2) ? face_of(colv[j], p) : -1;
+  }
+  __syncthreads();  // the face tables; no barrier after this
+  const int nbat = (nb + 7) / 8;
+  const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
+  double nar[3], nai[KS];
+  int ne = -1;
+  unsigned nfo = 0u;
+  unsigned long long nsm = 0ull, nem = 0ull;
+  auto load = [&](int bt) {
+    const int i = bt * 8 + g;
+    const bool ok = bt < b1 && i < nb;
+    const double *r = rec + (size_t)(ok ? i : 0) * RECW;
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) nar[ks] = ok ? r[ks * 4 + t4] : 0.0;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks)
+      nai[ks] = !ok ? 0.0 : FUSED ? (ks >= 3 ? r[ks * 4 + t4] : 0.0) : r[BK + ks * 4 + t4];
+    ne = ok ? list[i] : -1;
+    nfo = ne >= 0 ? fopack[ne] : 0u;
+    nsm = (MODE == 1 && ne >= 0) ? signmask[ne] : 0ull;
+    nem = (MODE == 1 && eliminate && ne >= 0) ? essmask[ne] : 0ull;
+  };
+  load(b0);
+  for (int bt = b0; bt < b1; ++bt) {
+    double ar[3], ai[KS];
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) ar[ks] = nar[ks];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) ai[ks] = nai[ks];
+    const int e = ne;
+    const unsigned fp = nfo;
+    const unsigned long long sm = nsm, em = nem;
+    load(bt + 1);
+    dcplx *base = e >= 0 ? Ae + (size_t)e * nd * rs : Ae;
+#pragma unroll
+    for (int j = 0; j < PB; ++j)
+      bulk_rowpair<CROSS, MODE, KS, FUSED>(bf[j], ar, ai, okv[j] && e >= 0, fp, sm, em, rowv[j],
+                                           colv[j], frv[j], fcv[j], sT, nd, rs, base);
   }
 }
 
@@ -712,16 +805,12 @@ __device__ __forceinline__ QCoef pml_qcoef(const PmlParams &pml, int rule, int m
   return c;
 }
 
-// One staged pair of PML rows: element-local columns k = 2 pr, 2 pr + 1 of
-// quadrature point q (chunk row block qi): physical shapes/curls, the dual
-// face transform, and X (real), Y = W X (two planes) at row stride LD.
-template <int LD>
-__device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule &R, int nd, int p,
-                                               int te, bool need_v, bool need_c, int rule, int rq,
-                                               const double *sJ, const double *sJi, double sidet,
-                                               unsigned sfo, const QCoef &C, double *Xs,
-                                               double *Yr, double *Yi) {
-  double v[2][3], c[2][3];
+// Physical shapes v and curls c of the element-local columns k = 2 pr,
+// 2 pr + 1 at quadrature point q, with the dual face transform applied.
+__device__ __forceinline__ void pml_shapes_pair(int pr, int q, const Rule &R, int p, int te,
+                                                bool need_v, bool need_c, const double *sJ,
+                                                const double *sJi, double sidet, unsigned sfo,
+                                                double (&v)[2][3], double (&c)[2][3]) {
   {
     // reference shapes / curls of columns 2 pr, 2 pr + 1 (zero past nd)
     double2 rv[3], rc[3];
@@ -753,7 +842,19 @@ __device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule
       }
     }
   }
-  
+}
+
+// One staged pair of PML rows: element-local columns k = 2 pr, 2 pr + 1 of
+// quadrature point q (chunk row block qi): physical shapes/curls, the dual
+// face transform, and X (real), Y = W X (two planes) at row stride LD.
+template <int LD>
+__device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule &R, int nd, int p,
+                                               int te, bool need_v, bool need_c, int rule, int rq,
+                                               const double *sJ, const double *sJi, double sidet,
+                                               unsigned sfo, const QCoef &C, double *Xs,
+                                               double *Yr, double *Yi) {
+  double v[2][3], c[2][3];
+  pml_shapes_pair(pr, q, R, p, te, need_v, need_c, sJ, sJi, sidet, sfo, v, c);
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int k = 2 * pr + h;
@@ -900,6 +1001,276 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
         dst[(size_t)row * rs + col + 1] = v2[1];
       } else if (col < nd) {
         dst[(size_t)row * rs + col] = v2[0];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PML elements with the element matrix split by symmetry (alternative to
+// k_pml_mma, chosen by the autotuner).
+//
+// Per mass-rule point the cross coefficients satisfy M1 = -M0^T entry by
+// entry (c02 = -b20, c12 = -b21, c20 = -b02, c21 = -b12: K is antisymmetric
+// and Lambda^-1 diagonal), so
+//   A_e = S + alpha P - beta P^T,   P_kl = sum_q v_k . (M0 c_l),
+// with S the complex-symmetric part (curl-curl with diagonal Lambda^-1, mass,
+// KLK) and alpha / beta the CROSS0 / CROSS1 selections.  Pass 1 contracts
+// all tiles of P (X = v, Y = M0 c) into shared memory; pass 2 contracts only
+// the tiles of S on or above the diagonal (X = c, Y = W c; X = v, Y = A v);
+// the epilogue writes each S tile and its mirror with the P terms added.
+// Every point stages 3 rows.  DMMA work at p = 3 with the cross terms:
+// (36 + 21) tiles x 3 rows per mass point and 21 x 3 per curl point, against
+// 36 x 6 and 36 x 3 in k_pml_mma; without them 21 of 36 tiles.
+//
+// The upper tiles are dealt to the warps in a folded order (column MT-1-j,
+// then column j, ...), so each warp's tiles lie in at most two columns and
+// the warps' tile counts differ by at most one.
+// ---------------------------------------------------------------------------
+template <int NDP8>
+struct PmlSymShape {
+  static constexpr int MT = NDP8 / 8;
+  static constexpr int LD = PmlShape<NDP8>::LD;
+  static constexpr int NT = MT * (MT + 1) / 2;      // tiles on or above the diagonal
+  static constexpr int TPW = (NT + MT - 1) / MT;    // most upper tiles of one warp
+  static constexpr int QS = NDP8 >= 48 ? 16 : 8;    // points per chunk (3 rows each)
+  // stage planes X, Yre, Yim of 3 QS rows, the coefficient table, and
+  // (with the cross terms) P as two planes of NDP8 rows
+  static size_t smem(int nq_all, bool cross) {
+    return (size_t)3 * (3 * QS) * LD * sizeof(double) + (size_t)nq_all * sizeof(QCoef) +
+           (cross ? (size_t)2 * NDP8 * LD * sizeof(double) : 0);
+  }
+};
+
+// Upper tile t of an MT x MT tile grid in the folded order.
+template <int MT>
+__host__ __device__ constexpr void sym_tile(int t, int &m, int &n) {
+  for (int j = 0; j < MT / 2; ++j) {
+    if (t < MT - j) { m = t; n = MT - 1 - j; return; }
+    t -= MT - j;
+    if (t < j + 1) { m = t; n = j; return; }
+    t -= j + 1;
+  }
+  m = t;
+  n = MT / 2;
+}
+
+// One staged pair of rows of the split kernel.  kind 0: curl-curl (X = c,
+// Y = diag(Lambda^-1 terms) c); 1: symmetric mass part (X = v, Y = A v);
+// 2: cross part (X = v, Y = M0 c).
+template <int LD>
+__device__ __forceinline__ void pml_sym_stage_pair(int qi, int pr, int q, const Rule &R, int p,
+                                                   int te, int kind, const double *sJ,
+                                                   const double *sJi, double sidet, unsigned sfo,
+                                                   const QCoef &C, double *Xs, double *Yr,
+                                                   double *Yi) {
+  double v[2][3], c[2][3];
+  pml_shapes_pair(pr, q, R, p, te, kind != 0, kind != 1, sJ, sJi, sidet, sfo, v, c);
+  const int rb = 3 * qi;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int k = 2 * pr + h;
+    dcplx y0, y1, y2;
+    const double *x;
+    if (kind == 0) {
+      x = c[h];
+      y0 = cscale(c[h][0], C.a00); y1 = cscale(c[h][1], C.a11); y2 = cscale(c[h][2], C.a22);
+    } else if (kind == 1) {
+      x = v[h];
+      y0 = cadd(cscale(v[h][0], C.a00), cscale(v[h][1], C.a01));
+      y1 = cadd(cscale(v[h][0], C.a10), cscale(v[h][1], C.a11));
+      y2 = cscale(v[h][2], C.a22);
+    } else {
+      x = v[h];
+      y0 = cscale(c[h][2], C.b02); y1 = cscale(c[h][2], C.b12);
+      y2 = cadd(cscale(c[h][0], C.b20), cscale(c[h][1], C.b21));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = x[d];
+    Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+    Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+    Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+  }
+}
+
+template <int NDP8, bool CROSS, int MODE>
+__global__ void __launch_bounds__(NDP8 * 4, PmlShape<NDP8>::MINB)
+k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc, Rule rm,
+          const double *__restrict__ J9, const double *__restrict__ Ji9,
+          const double *__restrict__ detJ, const double *__restrict__ v0,
+          const int *__restrict__ attr, const dcplx *__restrict__ eps_tab,
+          const dcplx *__restrict__ elem_eps, PmlParams pml, int mask_cc, int mask_mass,
+          int te, int eliminate, const unsigned *__restrict__ fopack,
+          const unsigned long long *__restrict__ signmask,
+          const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
+  using Sh = PmlSymShape<NDP8>;
+  constexpr int LD = Sh::LD, MT = Sh::MT, QS = Sh::QS, TPW = Sh::TPW;
+  extern __shared__ double smem[];
+  double *Xs = smem;
+  double *Yr = Xs + 3 * QS * LD;
+  double *Yi = Yr + 3 * QS * LD;
+  const int nq_all = rcc.nq + rm.nq;  // <= PML_MAXQ, checked by the host
+  QCoef *qtab = reinterpret_cast<QCoef *>(Yi + 3 * QS * LD);
+  double *Pr = reinterpret_cast<double *>(qtab + nq_all);
+  double *Pi = Pr + NDP8 * LD;
+  __shared__ double sJ[9], sJi[9], sidet;
+  __shared__ unsigned sfo;
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  constexpr int npair = NDP8 / 2;
+  const bool cross = CROSS && (mask_mass & 12);
+  // M0's coefficients are needed whenever either cross term is selected
+  const int mask_coef = cross ? (mask_mass | 4) : mask_mass;
+
+  // this warp's upper tiles: rows tm[i], column na or nb
+  int tm[TPW];
+  bool tok[TPW], tsec[TPW];
+  int na = -1, nb = -1;
+  {
+    const int t0 = w * Sh::NT / MT, t1 = (w + 1) * Sh::NT / MT;
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) {
+      int m = 0, n = 0;
+      tok[i] = t0 + i < t1;
+      if (tok[i]) sym_tile<MT>(t0 + i, m, n);
+      if (tok[i] && na < 0) na = n;
+      tsec[i] = tok[i] && n != na;
+      if (tsec[i]) nb = n;
+      tm[i] = m;
+    }
+    if (na < 0) na = 0;
+    if (nb < 0) nb = na;
+  }
+
+  for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
+    const int e = list[ie];
+    if (tid < 9) { sJ[tid] = J9[(size_t)e * 9 + tid]; sJi[tid] = Ji9[(size_t)e * 9 + tid]; }
+    if (tid == 0) { sidet = 1.0 / detJ[e]; sfo = fopack[e]; }
+    for (int j = tid; j < nq_all; j += blockDim.x) {
+      const int rule = j < rcc.nq ? 0 : 1;
+      const int q = rule == 0 ? j : j - rcc.nq;
+      const Rule &R = rule == 0 ? rcc : rm;
+      const double *Jz = J9 + (size_t)e * 9 + 6;
+      const double z = v0[(size_t)e * 3 + 2] + Jz[0] * R.ip[q * 3 + 0] +
+                       Jz[1] * R.ip[q * 3 + 1] + Jz[2] * R.ip[q * 3 + 2];
+      const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
+      qtab[j] = pml_qcoef(pml, rule, rule == 0 ? mask_cc : mask_coef, z, R.w[q] * detJ[e], eps);
+    }
+    __syncthreads();
+
+    // one pass over a rule's points in chunks of QS: stage 3 rows a point,
+    // then contract them (CONTRACT(r0) runs per 4-row k-step)
+    auto pass = [&](const Rule &R, const QCoef *qc, int kind, auto &&contract) {
+      for (int q0 = 0; q0 < R.nq; q0 += QS) {
+        const int nqc = min(QS, R.nq - q0);
+        const int nrows = 3 * nqc, nrows4 = (nrows + 3) & ~3;
+        for (int i = tid; i < (nrows4 - nrows) * LD; i += blockDim.x) {
+          const int r = nrows + i / LD, k = i % LD;
+          Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+        }
+        for (int it = tid; it < nqc * npair; it += blockDim.x) {
+          const int qi = it / npair, pr = it - qi * npair;
+          pml_sym_stage_pair<LD>(qi, pr, q0 + qi, R, p, te, kind, sJ, sJi, sidet, sfo,
+                                 qc[q0 + qi], Xs, Yr, Yi);
+        }
+        __syncthreads();
+        for (int r0 = 0; r0 < nrows4; r0 += 4) contract(r0);
+        __syncthreads();
+      }
+    };
+
+    // pass 1: P = sum v^T (M0 c), all tiles, warp w owns column tile w
+    if (cross) {
+      double pr_[MT][2], pi_[MT][2];
+#pragma unroll
+      for (int m = 0; m < MT; ++m) { pr_[m][0] = pr_[m][1] = pi_[m][0] = pi_[m][1] = 0.0; }
+      pass(rm, qtab + rcc.nq, 2, [&](int r0) {
+        const double br = Yr[(r0 + t4) * LD + w * 8 + g];
+        const double bi = Yi[(r0 + t4) * LD + w * 8 + g];
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+          const double a = Xs[(r0 + t4) * LD + m * 8 + g];
+          dmma(pr_[m][0], pr_[m][1], a, br);
+          dmma(pi_[m][0], pi_[m][1], a, bi);
+        }
+      });
+#pragma unroll
+      for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int k = m * 8 + g, l = w * 8 + 2 * t4 + i;
+          Pr[k * LD + l] = pr_[m][i];
+          Pi[k * LD + l] = pi_[m][i];
+        }
+    }
+
+    // pass 2: the upper tiles of S
+    double sr[TPW][2], si[TPW][2];
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) { sr[i][0] = sr[i][1] = si[i][0] = si[i][1] = 0.0; }
+    auto contract_s = [&](int r0) {
+      const double bar = Yr[(r0 + t4) * LD + na * 8 + g];
+      const double bai = Yi[(r0 + t4) * LD + na * 8 + g];
+      double bbr = bar, bbi = bai;
+      if (nb != na) {
+        bbr = Yr[(r0 + t4) * LD + nb * 8 + g];
+        bbi = Yi[(r0 + t4) * LD + nb * 8 + g];
+      }
+#pragma unroll
+      for (int i = 0; i < TPW; ++i) {
+        if (!tok[i]) continue;
+        const double a = Xs[(r0 + t4) * LD + tm[i] * 8 + g];
+        dmma(sr[i][0], sr[i][1], a, tsec[i] ? bbr : bar);
+        dmma(si[i][0], si[i][1], a, tsec[i] ? bbi : bai);
+      }
+    };
+    if (mask_cc) pass(rcc, qtab, 0, contract_s);
+    if (mask_mass) pass(rm, qtab + rcc.nq, 1, contract_s);
+    if (cross) __syncthreads();  // P complete before the epilogue reads it
+
+    // epilogue: entry (k, l) of each upper tile and its mirror (l, k)
+    const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
+    const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
+    const bool al = mask_mass & 4, be = mask_mass & 8;
+    dcplx *dst = Ae + (size_t)e * nd * rs;
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) {
+      if (!tok[i]) continue;
+      const int n = tsec[i] ? nb : na;
+      const int k = tm[i] * 8 + g;
+      dcplx up[2], lo[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int l = n * 8 + 2 * t4 + c;
+        double ur = sr[i][c], ui = si[i][c], lr = ur, li = ui;
+        if (cross) {
+          const double pkr = Pr[k * LD + l], pki = Pi[k * LD + l];
+          const double plr = Pr[l * LD + k], pli = Pi[l * LD + k];
+          if (al) { ur += pkr; ui += pki; lr += plr; li += pli; }
+          if (be) { ur -= plr; ui -= pli; lr -= pkr; li -= pki; }
+        }
+        if (MODE == 1) {
+          const double sg = ((((sm >> k) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
+          ur *= sg; ui *= sg; lr *= sg; li *= sg;
+          if (((em >> k) | (em >> l)) & 1ull) { ur = ui = lr = li = 0.0; }
+        }
+        up[c] = mk(ur, ui);
+        lo[c] = mk(lr, li);
+      }
+      const int l0 = n * 8 + 2 * t4;
+      if (k < nd) {
+        if (l0 + 1 < nd) {
+          dst[(size_t)k * rs + l0] = up[0];
+          dst[(size_t)k * rs + l0 + 1] = up[1];
+        } else if (l0 < nd) {
+          dst[(size_t)k * rs + l0] = up[0];
+        }
+      }
+      if (n != tm[i] && k < nd) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+          if (l0 + c < nd) dst[(size_t)(l0 + c) * rs + k] = lo[c];
       }
     }
   }

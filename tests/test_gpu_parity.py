@@ -225,9 +225,9 @@ def test_against_reference_cuda_kernels(kcase):
 
 
 @pytest.mark.parametrize("kcase", [("grating", 3, 6.0), ("hole", 2, 0.0), ("hole", 1, 6.0), ("slab", 3, 6.0)], ids=ids)
-@pytest.mark.parametrize("variant", [0, 1, 2], ids=["simt", "dmma4", "dmma2"])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4], ids=["simt", "dmma4", "dmma2", "nb4", "nb2"])
 def test_bulk_variants(kcase, variant):
-    """Both bulk-element kernels (the autotuner's candidates) match the oracle."""
+    """Every bulk-element kernel (the autotuner's candidates) matches the oracle."""
     c = case(*kcase) if kcase[0] != "slab" else configs.small_case("slab", 3, 6.0, seed=13, h=3.2)
     g = AsmGpuGlobal(c.prob)
     assert g.Init(c.ad, 0) and g.SetBulkVariant(variant)
@@ -246,6 +246,8 @@ def test_bulk_variants(kcase, variant):
 
 
 PML_WS_CASES = [("grating", 3, 6.0), ("hole", 3, 0.0), ("slab", 3, 6.0), ("poly", 3, 6.0)]
+PML_SYM_CASES = [("grating", 1, 6.0), ("hole", 2, 0.0), ("poly", 2, 6.0)] + PML_WS_CASES
+PML_VARIANT_CASES = ([(1, k) for k in PML_WS_CASES] + [(2, k) for k in PML_SYM_CASES])
 
 
 def _case_any(kind, p, theta):
@@ -256,18 +258,23 @@ def _case_any(kind, p, theta):
     return case(kind, p, theta)
 
 
-@pytest.mark.parametrize("kcase", PML_WS_CASES, ids=ids)
-def test_pml_ws_variant(kcase):
-    """The warp-specialised p = 3 PML kernel matches the oracle for every
-    integrator mask, with and without the transform, and assembled."""
+@pytest.mark.parametrize("variant,kcase", PML_VARIANT_CASES,
+                         ids=[f"v{v}-{ids(k)}" for v, k in PML_VARIANT_CASES])
+def test_pml_variant_parity(variant, kcase):
+    """The other PML kernels (1: warp-specialised, p = 3; 2: symmetric
+    split, every p) match the oracle for every integrator mask, with and
+    without the transform, and assembled.  The split kernel's cross part is
+    P - P^T only when both cross terms are selected: the single-term masks
+    check its alpha / beta selection."""
     c = _case_any(*kcase)
     g = AsmGpuGlobal(c.prob)
-    assert g.Init(c.ad, 0) and g.SetPmlVariant(1)
+    assert g.Init(c.ad, 0) and g.SetPmlVariant(variant)
     assert g.PathCounts()[1] > 0
     mm = MASS | ((CROSS0 | CROSS1 | KLK) if c.prob.has_kpar else 0)
     masks = [(CURLCURL, mm, True), (CURLCURL, mm, False), (CURLCURL, 0, False), (0, MASS, False)]
     if c.prob.has_kpar:
-        masks += [(0, CROSS0, False), (0, CROSS1, False), (0, KLK, False)]
+        masks += [(0, CROSS0, False), (0, CROSS1, False), (0, KLK, False),
+                  (CURLCURL, MASS | CROSS0, True), (0, MASS | CROSS1 | KLK, True)]
     for mcc, mmass, te in masks:
         assert g.ComputeLocal(mcc, mmass, te)
         assert rel(g.DownloadLocal(), oracle.local(c.ad, c.prob, mcc, mmass, te)) < TOL, (mcc, mmass)
@@ -276,7 +283,7 @@ def test_pml_ws_variant(kcase):
     for elim in (False, True):
         assert g.Assemble(elim)
         assert rel(g.DownloadValues(), oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, elim)) < TOL
-    assert g.PmlTuning()[0] == 1
+    assert g.PmlTuning()[0] == variant
 
 
 def test_pml_variant_selection():
@@ -284,11 +291,16 @@ def test_pml_variant_selection():
     g = AsmGpuGlobal(c.prob)
     assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Autotune()
     v, ms = g.PmlTuning()
-    assert v in (0, 1) and min(ms) > 0 and ms[v] == min(ms)
+    assert v in (0, 1, 2) and min(ms) > 0 and ms[v] == min(ms)
     c2 = case("grating", 2, 6.0)
-    g2 = AsmGpu(c2.prob)
+    g2 = AsmGpuGlobal(c2.prob)
     assert g2.Init(c2.ad, 0)
     assert not g2.SetPmlVariant(1) and g2.last_error[0] == 3
+    assert not g2.SetPmlVariant(3) and g2.last_error[0] == 1
+    # below p = 3 the warp-specialised kernel is not timed
+    assert g2.BuildGlobal(c2.ad.ess) and g2.Autotune()
+    v2, ms2 = g2.PmlTuning()
+    assert v2 in (0, 2) and ms2[1] == 0.0 and ms2[0] > 0 and ms2[2] > 0
 
 
 def test_autotuner_picks_a_variant():
@@ -296,7 +308,8 @@ def test_autotuner_picks_a_variant():
     g = AsmGpuGlobal(c.prob)
     assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
     v, ms = g.Tuning()
-    assert v in (0, 1, 2) and min(ms) > 0 and ms[v] == min(ms)
+    assert len(ms) == 5 and v in range(5) and min(ms) > 0 and ms[v] == min(ms)
+    assert not g.SetBulkVariant(5) and g.last_error[0] == 1
 
 
 def test_high_valence_row():
