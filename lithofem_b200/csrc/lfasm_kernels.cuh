@@ -684,6 +684,13 @@ k_bulk_mma_nb(int nb, const int *__restrict__ list, const double *__restrict__ r
   int ne = -1;
   unsigned nfo = 0u;
   unsigned long long nsm = 0ull, nem = 0ull;
+  // element of this lane one batch further ahead: the metadata loads of a
+  // batch index by it and so never wait for the list load
+  auto elem_of = [&](int bt) {
+    const int i = bt * 8 + g;
+    return (bt < b1 && i < nb) ? list[i] : -1;
+  };
+  int e_ahead = elem_of(b0);
   auto load = [&](int bt) {
     const int i = bt * 8 + g;
     const bool ok = bt < b1 && i < nb;
@@ -693,10 +700,11 @@ k_bulk_mma_nb(int nb, const int *__restrict__ list, const double *__restrict__ r
 #pragma unroll
     for (int ks = 0; ks < KS; ++ks)
       nai[ks] = !ok ? 0.0 : FUSED ? (ks >= 3 ? r[ks * 4 + t4] : 0.0) : r[BK + ks * 4 + t4];
-    ne = ok ? list[i] : -1;
+    ne = e_ahead;
     nfo = ne >= 0 ? fopack[ne] : 0u;
     nsm = (MODE == 1 && ne >= 0) ? signmask[ne] : 0ull;
     nem = (MODE == 1 && eliminate && ne >= 0) ? essmask[ne] : 0ull;
+    e_ahead = elem_of(bt + 1);
   };
   load(b0);
   for (int bt = b0; bt < b1; ++bt) {
@@ -1488,27 +1496,25 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
 // the unit diagonal of an essential row set.  Inlined twice so that the
 // shared-memory path keeps shared-memory instructions.
 template <bool RAW>
-__device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, int lane,
-                                           const int *__restrict__ ea_ptr,
-                                           const int *__restrict__ ea,
-                                           const uint16_t *__restrict__ off,
-                                           const int *__restrict__ Jc,
-                                           const dcplx *__restrict__ Ae, int nd, int rs,
-                                           const unsigned char *__restrict__ ess,
-                                           const double *__restrict__ sign,
-                                           const int *__restrict__ dof, int eliminate,
-                                           long long n_erows) {
+__device__ __forceinline__ void gather_row_q(dcplx *acc, int r, int rb, int nr, int lane,
+                                             int p0, int p1, bool row_ess,
+                                             const int *__restrict__ ea,
+                                             const uint16_t *__restrict__ off,
+                                             const int *__restrict__ Jc,
+                                             const dcplx *__restrict__ Ae, int nd, int rs,
+                                             const unsigned char *__restrict__ ess,
+                                             const double *__restrict__ sign,
+                                             const int *__restrict__ dof, int eliminate,
+                                             long long n_erows) {
   for (int j = lane; j < nr; j += 32) acc[j] = mk(0.0, 0.0);
   __syncwarp();
-  const bool row_ess = eliminate && ess[r];
-  const int p1 = ea_ptr[r + 1];
   if (!RAW && nd <= 16) {
     // short element rows (p = 1): 32 / nd row-list entries per pass, one
     // lane per (entry, column); their loads issue together, the additions
     // go entry by entry (two entries may share a slot)
     const int epi = 32 / nd;
     const int sub = lane / nd, b = lane - sub * nd;
-    for (int q0 = ea_ptr[r]; q0 < p1; q0 += epi) {
+    for (int q0 = p0; q0 < p1; q0 += epi) {
       const int pp = q0 + sub;
       dcplx v = mk(0.0, 0.0);
       int j = -1;
@@ -1526,7 +1532,7 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
       }
     }
   } else {
-    for (int pp = ea_ptr[r]; pp < p1; ++pp) {
+    for (int pp = p0; pp < p1; ++pp) {
       const int id = ea[pp];  // the same in every lane
       if (!LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) continue;
       const dcplx *src = Ae + (size_t)id * rs;
@@ -1558,6 +1564,21 @@ __device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, in
     acc[lo] = mk(1.0, 0.0);
   }
   __syncwarp();
+}
+
+template <bool RAW>
+__device__ __forceinline__ void gather_row(dcplx *acc, int r, int rb, int nr, int lane,
+                                           const int *__restrict__ ea_ptr,
+                                           const int *__restrict__ ea,
+                                           const uint16_t *__restrict__ off,
+                                           const int *__restrict__ Jc,
+                                           const dcplx *__restrict__ Ae, int nd, int rs,
+                                           const unsigned char *__restrict__ ess,
+                                           const double *__restrict__ sign,
+                                           const int *__restrict__ dof, int eliminate,
+                                           long long n_erows) {
+  gather_row_q<RAW>(acc, r, rb, nr, lane, ea_ptr[r], ea_ptr[r + 1], eliminate && ess[r], ea, off,
+                    Jc, Ae, nd, rs, ess, sign, dof, eliminate, n_erows);
 }
 
 // LONG = false: one warp per row r < n, accumulator in shared memory; rows
