@@ -855,7 +855,9 @@ __device__ __forceinline__ void pml_shapes_pair(int pr, int q, const Rule &R, in
 // One staged pair of PML rows: element-local columns k = 2 pr, 2 pr + 1 of
 // quadrature point q (chunk row block qi): physical shapes/curls, the dual
 // face transform, and X (real), Y = W X (two planes) at row stride LD.
-template <int LD>
+// PAIR: both columns of a row in one 16-byte store (the p = 3 kernels; at
+// lower p the narrower register budget keeps one store per entry).
+template <int LD, bool PAIR = true>
 __device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule &R, int nd, int p,
                                                int te, bool need_v, bool need_c, int rule, int rq,
                                                const double *sJ, const double *sJi, double sidet,
@@ -863,41 +865,90 @@ __device__ __forceinline__ void pml_stage_pair(int qi, int pr, int q, const Rule
                                                double *Yr, double *Yi) {
   double v[2][3], c[2][3];
   pml_shapes_pair(pr, q, R, p, te, need_v, need_c, sJ, sJi, sidet, sfo, v, c);
+  if constexpr (!PAIR) {
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int k = 2 * pr + h;
-    const int rb = qi * rq;
-    if (rule == 0) {
+    for (int h = 0; h < 2; ++h) {
+      const int k = 2 * pr + h;
+      const int rb = qi * rq;
+      if (rule == 0) {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
-      const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
-                  y2 = cscale(c[h][2], C.a22);
-      Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-      Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-      Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
-    } else {
-      const double *vv = v[h], *cc = c[h];
+        for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = c[h][d];
+        const dcplx y0 = cscale(c[h][0], C.a00), y1 = cscale(c[h][1], C.a11),
+                    y2 = cscale(c[h][2], C.a22);
+        Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+        Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+        Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+      } else {
+        const double *vv = v[h], *cc = c[h];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
-      dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
-      dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
-      dcplx y2 = cscale(vv[2], C.a22);
-      if (need_c) {
-        y0 = cadd(y0, cscale(cc[2], C.b02));
-        y1 = cadd(y1, cscale(cc[2], C.b12));
-        y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+        for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = vv[d];
+        dcplx y0 = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+        dcplx y1 = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+        dcplx y2 = cscale(vv[2], C.a22);
+        if (need_c) {
+          y0 = cadd(y0, cscale(cc[2], C.b02));
+          y1 = cadd(y1, cscale(cc[2], C.b12));
+          y2 = cadd(y2, cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
 #pragma unroll
-        for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
-        const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
-                    z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
-        Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
-        Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
-        Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
+          for (int d = 0; d < 3; ++d) Xs[(rb + 3 + d) * LD + k] = cc[d];
+          const dcplx z0 = cscale(vv[2], C.c02), z1 = cscale(vv[2], C.c12),
+                      z2 = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+          Yr[(rb + 3) * LD + k] = z0.re; Yi[(rb + 3) * LD + k] = z0.im;
+          Yr[(rb + 4) * LD + k] = z1.re; Yi[(rb + 4) * LD + k] = z1.im;
+          Yr[(rb + 5) * LD + k] = z2.re; Yi[(rb + 5) * LD + k] = z2.im;
+        }
+        Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
+        Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
+        Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
       }
-      Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-      Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-      Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
     }
+    return;
+  }
+  // row d of both columns: one 16-byte store a plane (columns 2 pr,
+  // 2 pr + 1 side by side, LD even); the shape rows first, then (cross
+  // terms) the curl rows
+  const int o = qi * rq * LD + 2 * pr;
+  auto put = [&](int d, double x0, double x1, dcplx y0, dcplx y1) {
+    *reinterpret_cast<double2 *>(Xs + o + d * LD) = make_double2(x0, x1);
+    *reinterpret_cast<double2 *>(Yr + o + d * LD) = make_double2(y0.re, y1.re);
+    *reinterpret_cast<double2 *>(Yi + o + d * LD) = make_double2(y0.im, y1.im);
+  };
+  if (rule == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const dcplx a = d == 0 ? C.a00 : d == 1 ? C.a11 : C.a22;
+      put(d, c[0][d], c[1][d], cscale(c[0][d], a), cscale(c[1][d], a));
+    }
+    return;
+  }
+  {
+    dcplx y[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double *vv = v[h], *cc = c[h];
+      y[h][0] = cadd(cscale(vv[0], C.a00), cscale(vv[1], C.a01));
+      y[h][1] = cadd(cscale(vv[0], C.a10), cscale(vv[1], C.a11));
+      y[h][2] = cscale(vv[2], C.a22);
+      if (need_c) {
+        y[h][0] = cadd(y[h][0], cscale(cc[2], C.b02));
+        y[h][1] = cadd(y[h][1], cscale(cc[2], C.b12));
+        y[h][2] = cadd(y[h][2], cadd(cscale(cc[0], C.b20), cscale(cc[1], C.b21)));
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) put(d, v[0][d], v[1][d], y[0][d], y[1][d]);
+  }
+  if (need_c) {
+    dcplx z[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double *vv = v[h];
+      z[h][0] = cscale(vv[2], C.c02);
+      z[h][1] = cscale(vv[2], C.c12);
+      z[h][2] = cadd(cscale(vv[0], C.c20), cscale(vv[1], C.c21));
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) put(3 + d, c[0][d], c[1][d], z[0][d], z[1][d]);
   }
 }
 
@@ -913,7 +964,7 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
   using Sh = PmlShape<NDP8>;
   constexpr int LD = Sh::LD, MT = Sh::MT, QC = Sh::QC, RMAX = 6 * QC;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *Xs = smem;
   double *Yr = Xs + RMAX * LD;
   double *Yi = Yr + RMAX * LD;
@@ -965,8 +1016,8 @@ k_pml_mma(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
         }
         for (int it = tid; it < nqc * npair; it += blockDim.x) {
           const int qi = it / npair, pr = it - qi * npair;
-          pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, sJ, sJi,
-                             sidet, sfo, qc[q0 + qi], Xs, Yr, Yi);
+          pml_stage_pair<LD, (NDP8 >= 48)>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule,
+                                           rq, sJ, sJi, sidet, sfo, qc[q0 + qi], Xs, Yr, Yi);
         }
         __syncthreads();
         // tensor-core contraction of the staged rows
@@ -1074,30 +1125,35 @@ __device__ __forceinline__ void pml_sym_stage_pair(int qi, int pr, int q, const 
                                                    double *Yi) {
   double v[2][3], c[2][3];
   pml_shapes_pair(pr, q, R, p, te, kind != 0, kind != 1, sJ, sJi, sidet, sfo, v, c);
-  const int rb = 3 * qi;
+  double x[2][3];
+  dcplx y[2][3];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const int k = 2 * pr + h;
-    dcplx y0, y1, y2;
-    const double *x;
     if (kind == 0) {
-      x = c[h];
-      y0 = cscale(c[h][0], C.a00); y1 = cscale(c[h][1], C.a11); y2 = cscale(c[h][2], C.a22);
-    } else if (kind == 1) {
-      x = v[h];
-      y0 = cadd(cscale(v[h][0], C.a00), cscale(v[h][1], C.a01));
-      y1 = cadd(cscale(v[h][0], C.a10), cscale(v[h][1], C.a11));
-      y2 = cscale(v[h][2], C.a22);
-    } else {
-      x = v[h];
-      y0 = cscale(c[h][2], C.b02); y1 = cscale(c[h][2], C.b12);
-      y2 = cadd(cscale(c[h][0], C.b20), cscale(c[h][1], C.b21));
-    }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) Xs[(rb + d) * LD + k] = x[d];
-    Yr[(rb + 0) * LD + k] = y0.re; Yi[(rb + 0) * LD + k] = y0.im;
-    Yr[(rb + 1) * LD + k] = y1.re; Yi[(rb + 1) * LD + k] = y1.im;
-    Yr[(rb + 2) * LD + k] = y2.re; Yi[(rb + 2) * LD + k] = y2.im;
+      for (int d = 0; d < 3; ++d) x[h][d] = c[h][d];
+      y[h][0] = cscale(c[h][0], C.a00); y[h][1] = cscale(c[h][1], C.a11);
+      y[h][2] = cscale(c[h][2], C.a22);
+    } else if (kind == 1) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[h][d] = v[h][d];
+      y[h][0] = cadd(cscale(v[h][0], C.a00), cscale(v[h][1], C.a01));
+      y[h][1] = cadd(cscale(v[h][0], C.a10), cscale(v[h][1], C.a11));
+      y[h][2] = cscale(v[h][2], C.a22);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[h][d] = v[h][d];
+      y[h][0] = cscale(c[h][2], C.b02); y[h][1] = cscale(c[h][2], C.b12);
+      y[h][2] = cadd(cscale(c[h][0], C.b20), cscale(c[h][1], C.b21));
+    }
+  }
+  // columns 2 pr, 2 pr + 1 side by side: one 16-byte store a row (LD even)
+  const int o = 3 * qi * LD + 2 * pr;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    *reinterpret_cast<double2 *>(Xs + o + d * LD) = make_double2(x[0][d], x[1][d]);
+    *reinterpret_cast<double2 *>(Yr + o + d * LD) = make_double2(y[0][d].re, y[1][d].re);
+    *reinterpret_cast<double2 *>(Yi + o + d * LD) = make_double2(y[0][d].im, y[1][d].im);
   }
 }
 
@@ -1113,7 +1169,7 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae) {
   using Sh = PmlSymShape<NDP8>;
   constexpr int LD = Sh::LD, MT = Sh::MT, QS = Sh::QS, TPW = Sh::TPW;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *Xs = smem;
   double *Yr = Xs + 3 * QS * LD;
   double *Yi = Yr + 3 * QS * LD;
