@@ -1093,11 +1093,14 @@ struct PmlSymShape {
   static constexpr int NT = MT * (MT + 1) / 2;      // tiles on or above the diagonal
   static constexpr int TPW = (NT + MT - 1) / MT;    // most upper tiles of one warp
   static constexpr int QS = NDP8 >= 48 ? 16 : 8;    // points per chunk (3 rows each)
+  // P row stride: odd, so that the fragment-ordered stores and the
+  // transposed reads of P spread over the banks
+  static constexpr int LDP = LD + 1;
   // stage planes X, Yre, Yim of 3 QS rows, the coefficient table, and
   // (with the cross terms) P as two planes of NDP8 rows
   static size_t smem(int nq_all, bool cross) {
     return (size_t)3 * (3 * QS) * LD * sizeof(double) + (size_t)nq_all * sizeof(QCoef) +
-           (cross ? (size_t)2 * NDP8 * LD * sizeof(double) : 0);
+           (cross ? (size_t)2 * NDP8 * LDP * sizeof(double) : 0);
   }
 };
 
@@ -1176,7 +1179,8 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
   const int nq_all = rcc.nq + rm.nq;  // <= PML_MAXQ, checked by the host
   QCoef *qtab = reinterpret_cast<QCoef *>(Yi + 3 * QS * LD);
   double *Pr = reinterpret_cast<double *>(qtab + nq_all);
-  double *Pi = Pr + NDP8 * LD;
+  constexpr int LDP = Sh::LDP;
+  double *Pi = Pr + NDP8 * LDP;
   __shared__ double sJ[9], sJi[9], sidet;
   __shared__ unsigned sfo;
 
@@ -1264,8 +1268,8 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
           const int k = m * 8 + g, l = w * 8 + 2 * t4 + i;
-          Pr[k * LD + l] = pr_[m][i];
-          Pi[k * LD + l] = pi_[m][i];
+          Pr[k * LDP + l] = pr_[m][i];
+          Pi[k * LDP + l] = pi_[m][i];
         }
     }
 
@@ -1309,8 +1313,8 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
         const int l = n * 8 + 2 * t4 + c;
         double ur = sr[i][c], ui = si[i][c], lr = ur, li = ui;
         if (cross) {
-          const double pkr = Pr[k * LD + l], pki = Pi[k * LD + l];
-          const double plr = Pr[l * LD + k], pli = Pi[l * LD + k];
+          const double pkr = Pr[k * LDP + l], pki = Pi[k * LDP + l];
+          const double plr = Pr[l * LDP + k], pli = Pi[l * LDP + k];
           if (al) { ur += pkr; ui += pki; lr += plr; li += pli; }
           if (be) { ur -= plr; ui -= pli; lr -= pkr; li -= pki; }
         }
@@ -1342,17 +1346,21 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 
 // ---------------------------------------------------------------------------
 // PML elements at p = 3, warp-specialised (alternative to k_pml_mma<48>,
-// chosen by the autotuner).  Four producer warps stage the rows of chunk
-// c + 1 into one half of a double buffer while twelve consumer warps run the
-// DMMA contraction of chunk c from the other half; each consumer warp owns
-// three row tiles of one 8-column tile (real and imaginary planes).  The
+// chosen by the autotuner).  WS_PROD producer warps stage the rows of chunk
+// c + 1 into one half of a double buffer while WS_CONS consumer warps run
+// the DMMA contraction of chunk c from the other half; each consumer warp
+// owns a block of WS_CM x WS_CN of the 6 x 6 tiles (real and imaginary
+// planes), one consumer per SM sub-partition.  Staging takes more
+// instructions than the contraction, so most of the warps are producers.
+// The
 // halves are handed over through mbarriers (full: every producer thread
 // arrives after its stores; empty: every consumer thread arrives after its
 // loads).  Every wait is bounded: a wait that runs out sets *err, and that
 // thread then skips its remaining waits but keeps to the same loop, so the
 // kernel always finishes (with the error reported, results undefined).
 // ---------------------------------------------------------------------------
-constexpr int WS_CONS = 12, WS_PROD = 4;
+constexpr int WS_CM = 3, WS_CN = 3;  // row / column tiles per consumer warp
+constexpr int WS_CONS = (6 / WS_CM) * (6 / WS_CN), WS_PROD = 16 - WS_CONS;
 constexpr int WS_THREADS = (WS_CONS + WS_PROD) * 32;
 constexpr long long WS_WAIT_LIMIT = 1ll << 20;  // try_wait rounds before giving up
 
@@ -1477,13 +1485,15 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
 
   // -------------------------------------------------------------- consumers
   const int g = lane >> 2, t4 = lane & 3;
-  const int nt = warp % 6, mh = warp / 6;  // column tile, row-tile half
+  const int m0 = (warp / (6 / WS_CN)) * WS_CM, n0 = (warp % (6 / WS_CN)) * WS_CN;
   unsigned c = 0;
   for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
     const int e = list[ie];
-    double cr[3][2], ci[3][2];
+    double cr[WS_CM][WS_CN][2], ci[WS_CM][WS_CN][2];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) { cr[m][0] = cr[m][1] = ci[m][0] = ci[m][1] = 0.0; }
+    for (int m = 0; m < WS_CM; ++m)
+#pragma unroll
+      for (int n = 0; n < WS_CN; ++n) cr[m][n][0] = cr[m][n][1] = ci[m][n][0] = ci[m][n][1] = 0.0;
     for (int rule = 0; rule < 2; ++rule) {
       const int mask = rule == 0 ? mask_cc : mask_mass;
       if (!mask) continue;
@@ -1499,32 +1509,41 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
         const double *Yr = Xs + RMAX * LD;
         const double *Yi = Yr + RMAX * LD;
         for (int r0 = 0; r0 < nrows4; r0 += 4) {
-          const double br = Yr[(r0 + t4) * LD + nt * 8 + g];
-          const double bi = Yi[(r0 + t4) * LD + nt * 8 + g];
+          double br[WS_CN], bi[WS_CN];
 #pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            const double a = Xs[(r0 + t4) * LD + (mh * 3 + m) * 8 + g];
-            dmma(cr[m][0], cr[m][1], a, br);
-            dmma(ci[m][0], ci[m][1], a, bi);
+          for (int n = 0; n < WS_CN; ++n) {
+            br[n] = Yr[(r0 + t4) * LD + (n0 + n) * 8 + g];
+            bi[n] = Yi[(r0 + t4) * LD + (n0 + n) * 8 + g];
+          }
+#pragma unroll
+          for (int m = 0; m < WS_CM; ++m) {
+            const double a = Xs[(r0 + t4) * LD + (m0 + m) * 8 + g];
+#pragma unroll
+            for (int n = 0; n < WS_CN; ++n) {
+              dmma(cr[m][n][0], cr[m][n][1], a, br[n]);
+              dmma(ci[m][n][0], ci[m][n][1], a, bi[n]);
+            }
           }
         }
         mbar_arrive(&empty[b]);
       }
     }
-    // epilogue: C[row = (3 mh + m) 8 + g][col = 8 nt + 2 t4 + i]
+    // epilogue: C[row = (m0 + m) 8 + g][col = (n0 + n) 8 + 2 t4 + i]
     const unsigned long long sm = MODE == 1 ? signmask[e] : 0ull;
     const unsigned long long em = (MODE == 1 && eliminate) ? essmask[e] : 0ull;
     dcplx *dst = Ae + (size_t)e * nd * rs;
-    const int col = nt * 8 + 2 * t4;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      const int row = (mh * 3 + m) * 8 + g;
+    for (int m = 0; m < WS_CM; ++m)
+#pragma unroll
+    for (int n = 0; n < WS_CN; ++n) {
+      const int row = (m0 + m) * 8 + g;
+      const int col = (n0 + n) * 8 + 2 * t4;
       if (row >= nd) continue;
       dcplx v2[2];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int l = col + i;
-        double re = cr[m][i], im = ci[m][i];
+        double re = cr[m][n][i], im = ci[m][n][i];
         if (MODE == 1) {
           const double sg = ((((sm >> row) ^ (sm >> l)) & 1ull) ? -1.0 : 1.0);
           re *= sg; im *= sg;
