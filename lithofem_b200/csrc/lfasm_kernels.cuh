@@ -1346,21 +1346,21 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 
 // ---------------------------------------------------------------------------
 // PML elements at p = 3, warp-specialised (alternative to k_pml_mma<48>,
-// chosen by the autotuner).  WS_PROD producer warps stage the rows of chunk
-// c + 1 into one half of a double buffer while WS_CONS consumer warps run
-// the DMMA contraction of chunk c from the other half; each consumer warp
-// owns a block of WS_CM x WS_CN of the 6 x 6 tiles (real and imaginary
-// planes), one consumer per SM sub-partition.  Staging takes more
-// instructions than the contraction, so most of the warps are producers.
-// The
-// halves are handed over through mbarriers (full: every producer thread
-// arrives after its stores; empty: every consumer thread arrives after its
-// loads).  Every wait is bounded: a wait that runs out sets *err, and that
+// chosen by the autotuner).  WS_PROD producer warps stage the rows of the
+// next chunks into a ring of WS_NBUF buffers while WS_CONS consumer warps
+// run the DMMA contraction of the oldest one; each consumer warp owns a
+// block of WS_CM x WS_CN of the 6 x 6 tiles (real and imaginary planes),
+// one consumer per SM sub-partition.  Staging takes more instructions than
+// the contraction, so most of the warps are producers.  The buffers are
+// handed over through mbarriers (full: every producer thread arrives after
+// its stores; empty: every consumer thread arrives after its loads).
+// Every wait is bounded: a wait that runs out sets *err, and that
 // thread then skips its remaining waits but keeps to the same loop, so the
 // kernel always finishes (with the error reported, results undefined).
 // ---------------------------------------------------------------------------
 constexpr int WS_CM = 3, WS_CN = 3;  // row / column tiles per consumer warp
 constexpr int WS_CONS = (6 / WS_CM) * (6 / WS_CN), WS_PROD = 16 - WS_CONS;
+constexpr int WS_NBUF = 3;  // staging buffers in the ring
 constexpr int WS_THREADS = (WS_CONS + WS_PROD) * 32;
 constexpr long long WS_WAIT_LIMIT = 1ll << 20;  // try_wait rounds before giving up
 
@@ -1397,7 +1397,7 @@ struct PmlWsShape {
   static constexpr int NDP8 = 48, LD = 52, MT = 6, QC = 8, RMAX = 6 * QC;
   static constexpr size_t BUF = (size_t)3 * RMAX * LD;  // doubles per buffer half
   static size_t smem(int nq_all) {
-    return 2 * BUF * sizeof(double) + (size_t)nq_all * sizeof(QCoef);
+    return WS_NBUF * BUF * sizeof(double) + (size_t)nq_all * sizeof(QCoef);
   }
 };
 
@@ -1415,16 +1415,16 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
   using Sh = PmlWsShape;
   constexpr int LD = Sh::LD, QC = Sh::QC, RMAX = Sh::RMAX, NDP8 = Sh::NDP8;
   extern __shared__ double smem[];
-  QCoef *qtab = reinterpret_cast<QCoef *>(smem + 2 * Sh::BUF);
-  __shared__ unsigned long long full[2], empty[2];
+  QCoef *qtab = reinterpret_cast<QCoef *>(smem + WS_NBUF * Sh::BUF);
+  __shared__ unsigned long long full[WS_NBUF], empty[WS_NBUF];
   __shared__ double sJ[9], sJi[9], sidet;
   __shared__ unsigned sfo;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    mbar_init(&full[0], WS_PROD * 32);
-    mbar_init(&full[1], WS_PROD * 32);
-    mbar_init(&empty[0], WS_CONS * 32);
-    mbar_init(&empty[1], WS_CONS * 32);
+    for (int b = 0; b < WS_NBUF; ++b) {
+      mbar_init(&full[b], WS_PROD * 32);
+      mbar_init(&empty[b], WS_CONS * 32);
+    }
   }
   __syncthreads();
   const int nq_all = rcc.nq + rm.nq;
@@ -1461,7 +1461,7 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
         for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
           const int nqc = min(QC, R.nq - q0);
           const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
-          const unsigned b = c & 1u, use = c >> 1;
+          const unsigned b = c % WS_NBUF, use = c / WS_NBUF;
           if (live) live = mbar_wait(&empty[b], (use & 1u) ^ 1u, err);
           double *Xs = smem + b * Sh::BUF;
           double *Yr = Xs + RMAX * LD;
@@ -1503,7 +1503,7 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
       for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
         const int nqc = min(QC, R.nq - q0);
         const int nrows4 = (nqc * rq + 3) & ~3;
-        const unsigned b = c & 1u, use = c >> 1;
+        const unsigned b = c % WS_NBUF, use = c / WS_NBUF;
         if (live) live = mbar_wait(&full[b], use & 1u, err);
         const double *Xs = smem + b * Sh::BUF;
         const double *Yr = Xs + RMAX * LD;
