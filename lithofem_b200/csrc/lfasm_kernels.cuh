@@ -1361,6 +1361,11 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 constexpr int WS_CM = 3, WS_CN = 3;  // row / column tiles per consumer warp
 constexpr int WS_CONS = (6 / WS_CM) * (6 / WS_CN), WS_PROD = 16 - WS_CONS;
 constexpr int WS_NBUF = 3;  // staging buffers in the ring
+// producer threads that stage rows (one column pair each of a full chunk of
+// 8 points x 24 pairs); the other producer threads form the next element's
+// coefficient table meanwhile
+constexpr int WS_STAGE = 8 * 24;
+static_assert(WS_STAGE < WS_PROD * 32, "no producer threads left for the table");
 constexpr int WS_THREADS = (WS_CONS + WS_PROD) * 32;
 constexpr long long WS_WAIT_LIMIT = 1ll << 20;  // try_wait rounds before giving up
 
@@ -1395,9 +1400,10 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 
 struct PmlWsShape {
   static constexpr int NDP8 = 48, LD = 52, MT = 6, QC = 8, RMAX = 6 * QC;
-  static constexpr size_t BUF = (size_t)3 * RMAX * LD;  // doubles per buffer half
+  static constexpr size_t BUF = (size_t)3 * RMAX * LD;  // doubles per ring buffer
+  // the ring, then two coefficient tables (this element's, the next one's)
   static size_t smem(int nq_all) {
-    return WS_NBUF * BUF * sizeof(double) + (size_t)nq_all * sizeof(QCoef);
+    return WS_NBUF * BUF * sizeof(double) + (size_t)2 * nq_all * sizeof(QCoef);
   }
 };
 
@@ -1415,14 +1421,14 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
   using Sh = PmlWsShape;
   constexpr int LD = Sh::LD, QC = Sh::QC, RMAX = Sh::RMAX, NDP8 = Sh::NDP8;
   extern __shared__ double smem[];
-  QCoef *qtab = reinterpret_cast<QCoef *>(smem + WS_NBUF * Sh::BUF);
+  QCoef *qtab = reinterpret_cast<QCoef *>(smem + WS_NBUF * Sh::BUF);  // [2][nq_all]
   __shared__ unsigned long long full[WS_NBUF], empty[WS_NBUF];
-  __shared__ double sJ[9], sJi[9], sidet;
-  __shared__ unsigned sfo;
+  __shared__ double sJ[2][9], sJi[2][9], sidet[2];
+  __shared__ unsigned sfo[2];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
     for (int b = 0; b < WS_NBUF; ++b) {
-      mbar_init(&full[b], WS_PROD * 32);
+      mbar_init(&full[b], WS_STAGE);
       mbar_init(&empty[b], WS_CONS * 32);
     }
   }
@@ -1432,53 +1438,80 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
 
   if (warp >= WS_CONS) {
     // ------------------------------------------------------------ producers
+    // Element tables in two slots.  Producer threads 0 .. WS_STAGE - 1 stage
+    // the current element's rows (one column pair each) and alone arrive on
+    // the chunk barriers; the other producer threads form the next
+    // element's coefficient table and geometry in the other slot meanwhile.
+    // One producer barrier an element makes the new slot visible and frees
+    // the old one.
     const int ptid = tid - WS_CONS * 32;
     constexpr int npair = NDP8 / 2;
-    unsigned c = 0;
-    for (int ie = blockIdx.x; ie < npml; ie += gridDim.x) {
+    static_assert(QC * npair == WS_STAGE, "one column pair a staging thread");
+    constexpr int NFILL = WS_PROD * 32 - WS_STAGE;
+    const int nfill_items = max(nq_all, 9);
+    auto fill = [&](int ie, int slot, int t) {
       const int e = list[ie];
-      if (ptid < 9) { sJ[ptid] = J9[(size_t)e * 9 + ptid]; sJi[ptid] = Ji9[(size_t)e * 9 + ptid]; }
-      if (ptid == 0) { sidet = 1.0 / detJ[e]; sfo = fopack[e]; }
-      for (int j = ptid; j < nq_all; j += WS_PROD * 32) {
-        const int rule = j < rcc.nq ? 0 : 1;
-        const int q = rule == 0 ? j : j - rcc.nq;
+      if (t < 9) {
+        sJ[slot][t] = J9[(size_t)e * 9 + t];
+        sJi[slot][t] = Ji9[(size_t)e * 9 + t];
+      }
+      if (t == 0) { sidet[slot] = 1.0 / detJ[e]; sfo[slot] = fopack[e]; }
+      if (t < nq_all) {
+        const int rule = t < rcc.nq ? 0 : 1;
+        const int q = rule == 0 ? t : t - rcc.nq;
         const Rule &R = rule == 0 ? rcc : rm;
         const double *Jz = J9 + (size_t)e * 9 + 6;
         const double z = v0[(size_t)e * 3 + 2] + Jz[0] * R.ip[q * 3 + 0] +
                          Jz[1] * R.ip[q * 3 + 1] + Jz[2] * R.ip[q * 3 + 2];
         const dcplx eps = elem_eps ? elem_eps[e] : eps_tab[attr[e] - 1];
-        qtab[j] = pml_qcoef(pml, rule, rule == 0 ? mask_cc : mask_mass, z, R.w[q] * detJ[e], eps);
+        qtab[slot * nq_all + t] =
+            pml_qcoef(pml, rule, rule == 0 ? mask_cc : mask_mass, z, R.w[q] * detJ[e], eps);
       }
-      asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // producers only
-      for (int rule = 0; rule < 2; ++rule) {
-        const int mask = rule == 0 ? mask_cc : mask_mass;
-        if (!mask) continue;
-        const Rule R = rule == 0 ? rcc : rm;
-        const QCoef *qc = qtab + (rule == 0 ? 0 : rcc.nq);
-        const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
-        const bool need_v = rule == 1;
-        const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
-        for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
-          const int nqc = min(QC, R.nq - q0);
-          const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
-          const unsigned b = c % WS_NBUF, use = c / WS_NBUF;
-          if (live) live = mbar_wait(&empty[b], (use & 1u) ^ 1u, err);
-          double *Xs = smem + b * Sh::BUF;
-          double *Yr = Xs + RMAX * LD;
-          double *Yi = Yr + RMAX * LD;
-          for (int i = ptid; i < (nrows4 - nrows) * LD; i += WS_PROD * 32) {
-            const int r = nrows + i / LD, k = i % LD;
-            Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+    };
+    if (blockIdx.x < npml)
+      for (int t = ptid; t < nfill_items; t += WS_PROD * 32) fill(blockIdx.x, 0, t);
+    asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // producers only
+    unsigned c = 0;
+    int slot = 0;
+    for (int ie = blockIdx.x; ie < npml; ie += gridDim.x, slot ^= 1) {
+      if (ptid >= WS_STAGE) {
+        const int ien = ie + gridDim.x;
+        if (ien < npml)
+          for (int t = ptid - WS_STAGE; t < nfill_items; t += NFILL) fill(ien, slot ^ 1, t);
+      } else {
+        const double *tJ = sJ[slot], *tJi = sJi[slot];
+        const double tdet = sidet[slot];
+        const unsigned tfo = sfo[slot];
+        for (int rule = 0; rule < 2; ++rule) {
+          const int mask = rule == 0 ? mask_cc : mask_mass;
+          if (!mask) continue;
+          const Rule R = rule == 0 ? rcc : rm;
+          const QCoef *qc = qtab + slot * nq_all + (rule == 0 ? 0 : rcc.nq);
+          const bool need_c = rule == 0 ? true : (CROSS && (mask & (4 | 8)));
+          const bool need_v = rule == 1;
+          const int rq = rule == 0 ? 3 : (need_c ? 6 : 3);
+          for (int q0 = 0; q0 < R.nq; q0 += QC, ++c) {
+            const int nqc = min(QC, R.nq - q0);
+            const int nrows = nqc * rq, nrows4 = (nrows + 3) & ~3;
+            const unsigned b = c % WS_NBUF, use = c / WS_NBUF;
+            if (live) live = mbar_wait(&empty[b], (use & 1u) ^ 1u, err);
+            double *Xs = smem + b * Sh::BUF;
+            double *Yr = Xs + RMAX * LD;
+            double *Yi = Yr + RMAX * LD;
+            for (int i = ptid; i < (nrows4 - nrows) * LD; i += WS_STAGE) {
+              const int r = nrows + i / LD, k = i % LD;
+              Xs[r * LD + k] = 0.0; Yr[r * LD + k] = 0.0; Yi[r * LD + k] = 0.0;
+            }
+            if (ptid < nqc * npair) {
+              const int qi = ptid / npair, pr = ptid - qi * npair;
+              pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, tJ,
+                                 tJi, tdet, tfo, qc[q0 + qi], Xs, Yr, Yi);
+            }
+            mbar_arrive(&full[b]);
           }
-          for (int it = ptid; it < nqc * npair; it += WS_PROD * 32) {
-            const int qi = it / npair, pr = it - qi * npair;
-            pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, sJ, sJi,
-                               sidet, sfo, qc[q0 + qi], Xs, Yr, Yi);
-          }
-          mbar_arrive(&full[b]);
         }
       }
-      asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // table free again
+      asm volatile("bar.sync 1, %0;" ::"n"(WS_PROD * 32) : "memory");  // next slot ready
     }
     return;
   }
