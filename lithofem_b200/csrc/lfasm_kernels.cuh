@@ -1346,14 +1346,16 @@ k_pml_sym(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rc
 
 // ---------------------------------------------------------------------------
 // PML elements at p = 3, warp-specialised (alternative to k_pml_mma<48>,
-// chosen by the autotuner).  WS_PROD producer warps stage the rows of the
-// next chunks into a ring of WS_NBUF buffers while WS_CONS consumer warps
-// run the DMMA contraction of the oldest one; each consumer warp owns a
-// block of WS_CM x WS_CN of the 6 x 6 tiles (real and imaginary planes),
-// one consumer per SM sub-partition.  Staging takes more instructions than
-// the contraction, so most of the warps are producers.  The buffers are
-// handed over through mbarriers (full: every producer thread arrives after
-// its stores; empty: every consumer thread arrives after its loads).
+// chosen by the autotuner).  WS_PROD producer warps: WS_STAGE threads stage
+// the rows of the next chunks into a ring of WS_NBUF buffers, the others
+// form the next element's coefficient table in a second table slot; while
+// WS_CONS consumer warps run the DMMA contraction of the oldest buffer.
+// Each consumer warp owns a block of WS_CM x WS_CN of the 6 x 6 tiles (real
+// and imaginary planes), one consumer per SM sub-partition.  Staging takes
+// more instructions than the contraction, so most of the warps are
+// producers.  The buffers are handed over through mbarriers (full: every
+// staging thread arrives after its stores; empty: every consumer thread
+// arrives after its loads).
 // Every wait is bounded: a wait that runs out sets *err, and that
 // thread then skips its remaining waits but keeps to the same loop, so the
 // kernel always finishes (with the error reported, results undefined).
