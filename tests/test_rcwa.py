@@ -128,3 +128,27 @@ def test_line_grating_matches_rcwa(duty):
                   else bot.A * np.exp(1j * bot.qA * (z_ref - bot.zA)))
             eff = orders.order_efficiencies(oset, z, z_ref, direction, area, inc, bg00=bg)
             _compare(eff, ref["orders"], ref[side + "_eff"], GATE)
+
+
+def test_order_efficiencies_refer_each_order_to_the_reference_plane():
+    """In an absorbing medium an up-going order decays with height; sampled
+    at two heights, the efficiency referred to z_ref is the same, and equals
+    that of the amplitude the wave has at z_ref."""
+    lx, ly, k0, nx, ny = 20.0, 2.0, 2 * np.pi / 13.5, 8, 2
+    eps = 1.0 + 0.05j
+    kx0 = k0 * np.sin(np.deg2rad(6.0))
+    area = lx * ly
+    inc = orders.incident_flux(k0, 1.0, kx0, 0.0, area)
+    qz = orders.order_qz(k0, eps, kx0, 0.0)
+    assert qz.imag > 0
+    z_ref, a_ref = 10.0, 0.4 + 0.2j                # s-polarised amplitude at z_ref
+    got = []
+    for z in (4.0, 7.5):
+        a = a_ref * np.exp(1j * qz * (z - z_ref))  # up-going: e^{i qz z}
+        samples = np.zeros((ny, nx, 3), dtype=complex)
+        samples[..., 1] = a
+        oset = orders.orders_from_plane(samples, lx, ly, (kx0, 0.0), k0, eps)
+        got.append(orders.order_efficiencies(oset, z, z_ref, +1, area, inc)[(0, 0)])
+    c = np.array([0.0, a_ref, 0.0])
+    want = orders.plane_wave_flux(c, kx0, 0.0, qz, k0, +1, area) / inc
+    assert abs(got[0] - want) < 1e-13 * abs(want) and abs(got[1] - want) < 1e-13 * abs(want)
