@@ -139,3 +139,22 @@ def test_validation_of_large_arrays_reports_the_lowest_index():
     rc = _lib.lib().lfasm_init(ct.byref(m.ad), ct.byref(m.prob), 0, ct.byref(h))
     assert rc == 1 and _lib.lib().lfasm_last_error() == b"detJ[250001] not positive"
     del keep
+
+
+def test_tuning_entry_points_reject_a_null_handle():
+    """The variant setters and getters check their handle before anything
+    else; the header's variant count is the one the Python layer sizes its
+    buffers with."""
+    import re
+    from pathlib import Path
+    L = _lib.lib()
+    null = ct.c_void_p()
+    v = ct.c_int()
+    ms = (ct.c_float * _abi.BULK_VARIANTS)()
+    for rc in (L.lfasm_set_bulk_variant(null, 1), L.lfasm_set_pml_variant(null, 1),
+               L.lfasm_get_tuning(null, ct.byref(v), ms),
+               L.lfasm_get_pml_tuning(null, ct.byref(v), ms), L.lfasm_autotune(null)):
+        assert rc == 1 and b"NULL handle" in L.lfasm_last_error()
+    header = (Path(__file__).resolve().parents[1] / "include" / "lfasm.h").read_text()
+    n = int(re.search(r"#define LFASM_BULK_VARIANTS (\d+)", header).group(1))
+    assert n == _abi.BULK_VARIANTS == 5
