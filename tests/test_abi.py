@@ -158,3 +158,34 @@ def test_tuning_entry_points_reject_a_null_handle():
     header = (Path(__file__).resolve().parents[1] / "include" / "lfasm.h").read_text()
     n = int(re.search(r"#define LFASM_BULK_VARIANTS (\d+)", header).group(1))
     assert n == _abi.BULK_VARIANTS == 5
+
+
+def test_no_cpu_fallback(tmp_path):
+    """Without its library the Python layer raises on first use; with the
+    library but without a usable GPU, lfasm_init fails with a CUDA error
+    instead of computing anything on the host."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = ("from lithofem_b200 import configs\n"
+            "from lithofem_b200.asm import AsmGpu\n"
+            "c = configs.small_case('slab', 1, 0.0)\n"
+            "g = AsmGpu(c.prob)\n"
+            "try:\n"
+            "    ok = g.Init(c.ad, 0)\n"
+            "except RuntimeError as e:\n"
+            "    print('RAISED', e)\n"
+            "else:\n"
+            "    print('OK' if ok else 'FAILED', getattr(g, 'last_error', None))\n")
+    env = dict(os.environ, LFASM_LIBRARY=str(tmp_path / "absent.so"))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                         text=True, timeout=300).stdout
+    assert "RAISED" in out and "no CPU fallback" in out, out
+    import torch
+    if not torch.cuda.is_available():
+        env = {k: v for k, v in os.environ.items() if k != "LFASM_LIBRARY"}
+        out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env,
+                             capture_output=True, text=True, timeout=300).stdout
+        assert "FAILED (2," in out, out
