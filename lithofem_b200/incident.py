@@ -55,10 +55,12 @@ def sp_basis(theta: float, phi: float, from_top: bool):
 
 
 def kpar_of(stack: MeshStack, theta: float, phi: float = 0.0, from_top: bool = True):
-    """In-plane wavevector of a plane wave entering from the top (bottom) ambient."""
-    slabs = stack.slabs
-    eps_in = stack.eps_bg_of_slab(len(slabs) - 2 if from_top else 0)
-    kp = stack.k0 * math.sqrt(complex(eps_in).real) * math.sin(math.radians(theta))
+    """In-plane wavevector k0 sin(theta) (cos phi, sin phi) of a plane-wave
+    source: the reference defines a source's angle in vacuum whatever the
+    incidence ambient (src/lithofem/config.py:472-473), so ``from_top`` does
+    not enter."""
+    del from_top
+    kp = stack.k0 * math.sin(math.radians(theta))
     return (kp * math.cos(math.radians(phi)), kp * math.sin(math.radians(phi)))
 
 

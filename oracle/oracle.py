@@ -84,6 +84,10 @@ def ref() -> ct.CDLL:
         L.ref_ctx_gpu_local.restype = ct.c_int
         L.ref_ctx_gpu_global.argtypes = [ct.c_void_p, i, ct.c_int, ct.c_int, ct.c_int, d, d, d]
         L.ref_ctx_gpu_global.restype = ct.c_int
+        L.ref_ctx_set_csr.argtypes = [ct.c_void_p, i, ct.c_longlong, i]
+        L.ref_set_incident.argtypes = [ct.c_int, ct.c_int] + [d] * 8
+        L.ref_incident_at.argtypes = [ct.c_int, ct.c_double, d]
+        L.ref_scatter_source_elems.argtypes = [ct.c_int, i, d, d, ct.c_int, d, d]
         _ref = L
     return _ref
 
@@ -153,6 +157,66 @@ def rhs(ad: AsmData, prob: Problem, parts, col_of_part, ncol: int, ess, eliminat
 # reference build
 # ---------------------------------------------------------------------------
 
+def _c2(a) -> np.ndarray:
+    a = np.asarray(a, dtype=np.complex128)
+    return np.ascontiguousarray(np.stack([a.real, a.imag], axis=-1).reshape(-1))
+
+
+def ref_set_problem(prob: Problem, order: int) -> None:
+    """The reference's global problem (Problem/Region) from ours."""
+    regs = prob.regions
+    eps = _c2([r.eps for r in regs])
+    dl = _c2([r.delta_eps for r in regs])
+    kind = np.array([r.kind for r in regs], dtype=np.int32)
+    slab = np.array([r.slab for r in regs], dtype=np.int32)
+    ref().ref_set_problem(prob.k0, prob.kx, prob.ky, prob.z_min, prob.z_max, prob.pml_thick,
+                          prob.pml_order, prob.pml_target, order, len(regs),
+                          eps.ctypes.data_as(c_double_p), kind.ctypes.data_as(c_int_p),
+                          slab.ctypes.data_as(c_int_p), dl.ctypes.data_as(c_double_p))
+
+
+def ref_set_incident(parts) -> None:
+    """The reference's incident tables (prob.incident) from per-slab
+    SlabWave lists, one list per part; call after ref_set_problem."""
+    n_parts, n_slab = len(parts), len(parts[0])
+    zlo = np.array([sw.z_lo for sw in parts[0]], dtype=np.float64)
+    zhi = np.array([sw.z_hi for sw in parts[0]], dtype=np.float64)
+    flat = [sw for slabs in parts for sw in slabs]
+    qA, qB = _c2([sw.qA for sw in flat]), _c2([sw.qB for sw in flat])
+    zA = np.array([sw.zA for sw in flat], dtype=np.float64)
+    zB = np.array([sw.zB for sw in flat], dtype=np.float64)
+    A, B = _c2([sw.A for sw in flat]), _c2([sw.B for sw in flat])
+    ref().ref_set_incident(n_parts, n_slab, *[x.ctypes.data_as(c_double_p)
+                                              for x in (zlo, zhi, qA, qB, zA, zB, A, B)])
+
+
+def ref_incident_at(slab: int, z: float) -> np.ndarray:
+    out = np.empty(6)
+    ref().ref_incident_at(slab, z, out.ctypes.data_as(c_double_p))
+    return out.view(np.complex128)
+
+
+def ref_scatter_source(ad: AsmData, prob: Problem, parts, elements=None,
+                       rule=None) -> np.ndarray:
+    """The reference's ScatterSource::Eval (problem_common.inc:239-266) at
+    every point of ``rule`` (default: the mass rule) of the given elements:
+    (len(elements), nq, 3) complex."""
+    rule = ad.rule_mass if rule is None else rule
+    sel = np.arange(ad.ne) if elements is None else np.asarray(elements)
+    ref_set_problem(prob, ad.p)
+    ref_set_incident(parts)
+    attr = np.ascontiguousarray(ad.attr[sel], dtype=np.int32)
+    J = np.ascontiguousarray(ad.J.reshape(ad.ne, 9)[sel].reshape(-1))
+    v0 = np.ascontiguousarray(ad.v0.reshape(ad.ne, 3)[sel].reshape(-1))
+    ip = np.ascontiguousarray(np.asarray(rule.ip, dtype=np.float64).reshape(-1))
+    out = np.empty(len(sel) * rule.nq * 6)
+    ref().ref_scatter_source_elems(len(sel), attr.ctypes.data_as(c_int_p),
+                                   J.ctypes.data_as(c_double_p), v0.ctypes.data_as(c_double_p),
+                                   rule.nq, ip.ctypes.data_as(c_double_p),
+                                   out.ctypes.data_as(c_double_p))
+    return out.view(np.complex128).reshape(len(sel), rule.nq, 3)
+
+
 class RefContext:
     """The reference's AsmData + global problem, filled from our extraction."""
 
@@ -210,6 +274,14 @@ class RefContext:
         J = np.empty(self.nnz, dtype=np.int32)
         L.ref_ctx_get_csr(self.ctx, I.ctypes.data_as(c_int_p), J.ctypes.data_as(c_int_p))
         return I, J
+
+    def set_csr(self, I: np.ndarray, J: np.ndarray) -> None:
+        """Use a given CSR (height + 1 row pointer) instead of building one."""
+        I = np.ascontiguousarray(I, dtype=np.int32)
+        J = np.ascontiguousarray(J, dtype=np.int32)
+        ref().ref_ctx_set_csr(self.ctx, I.ctypes.data_as(c_int_p), len(J),
+                              J.ctypes.data_as(c_int_p))
+        self.nnz = len(J)
 
     def reassemble(self) -> np.ndarray:
         if self.nnz is None:

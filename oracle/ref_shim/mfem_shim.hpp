@@ -117,13 +117,24 @@ struct IntegrationRules {
 };
 static IntegrationRules IntRules;
 
+// Affine element map x = v0 + J xi, enough for the reference's coefficient
+// classes (ScatterSource::Eval calls Attribute and Transform); the Jacobian
+// queries of the MFEM extraction stay unavailable.
 class ElementTransformation {
  public:
   int Attribute = 0;
+  bool affine = false;
+  double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // row-major
+  double v0[3] = {0, 0, 0};
   void SetIntPoint(const IntegrationPoint *) { shim_unreachable("ElementTransformation"); }
   const DenseMatrix &Jacobian() { shim_unreachable("ElementTransformation"); }
   double Weight() { shim_unreachable("ElementTransformation"); }
-  void Transform(const IntegrationPoint &, Vector &) { shim_unreachable("ElementTransformation"); }
+  void Transform(const IntegrationPoint &ip, Vector &x) {
+    if (!affine) shim_unreachable("ElementTransformation::Transform");
+    const double xi[3] = {ip.x, ip.y, ip.z};
+    for (int i = 0; i < 3; ++i)
+      x(i) = v0[i] + J[3 * i] * xi[0] + J[3 * i + 1] * xi[1] + J[3 * i + 2] * xi[2];
+  }
 };
 
 class FiniteElement {

@@ -13,6 +13,10 @@
 //   ref_ctx_element       reassemble_element   (asm_data.inc:218-370)
 //   ref_ctx_gpu_local     AsmGpu::Init + ComputeLocal + DownloadLocal
 //   ref_ctx_gpu_global    AsmGpuGlobal::BuildGlobal + ScatterEliminate
+//   ref_ctx_set_csr       a caller-given CSR for the context (element shares)
+//   ref_set_incident      the incident tables of the global problem
+//   ref_incident_at       incident_at          (problem_common.inc:219-236)
+//   ref_scatter_source    ScatterSource::Eval  (problem_common.inc:239-266)
 //
 // Built by oracle/Makefile into oracle/_ref/libref_asm.so.
 #include <cuda_runtime.h>
@@ -171,6 +175,89 @@ int ref_ctx_gpu_local(void *ctx, int mask_cc, int mask_mass, int te, double *out
     if (!g.DownloadLocal(h)) return 3;
     std::memcpy(out, h.data(), h.size() * sizeof(DC));
   }
+  return 0;
+}
+
+// Replaces the context's CSR (height + 1 row pointer, nnz columns) with a
+// caller-given one: a share of the elements can then be reassembled into the
+// full rows of the mesh's own sparsity (rows the share does not touch empty).
+int ref_ctx_set_csr(void *ctx, const int *I, long long nnz, const int *J) {
+  AsmData *ad = static_cast<AsmData *>(ctx);
+  ad->I.assign(I, I + (size_t)ad->height + 1);
+  ad->Jcol.assign(J, J + (size_t)nnz);
+  return 0;
+}
+
+// Incident-field tables of the global problem (prob.incident, parts x slabs;
+// problem_common.inc:11-16, 43-57): n_parts * n_slab SlabWave records, part
+// major; qA/qB {re, im}, A/B 3 x {re, im} per record.  Call after
+// ref_set_problem, which resets the problem.
+int ref_set_incident(int n_parts, int n_slab, const double *z_lo, const double *z_hi,
+                     const double *qA, const double *qB, const double *zA, const double *zB,
+                     const double *A, const double *B) {
+  prob.incident.assign(n_parts, std::vector<SlabWave>(n_slab));
+  prob.active_parts.clear();
+  for (int p = 0; p < n_parts; ++p)
+    for (int s = 0; s < n_slab; ++s) {
+      const size_t r = (size_t)p * n_slab + s;
+      SlabWave &w = prob.incident[p][s];
+      w.z_lo = z_lo[s];
+      w.z_hi = z_hi[s];
+      w.zA = zA[r];
+      w.zB = zB[r];
+      w.qA = C(qA[2 * r], qA[2 * r + 1]);
+      w.qB = C(qB[2 * r], qB[2 * r + 1]);
+      for (int i = 0; i < 3; ++i) {
+        w.A[i] = C(A[6 * r + 2 * i], A[6 * r + 2 * i + 1]);
+        w.B[i] = C(B[6 * r + 2 * i], B[6 * r + 2 * i + 1]);
+      }
+    }
+  return 0;
+}
+
+// incident_at (problem_common.inc:219-236): Ehat(z) in slab `slab`, summed
+// over the parts; out = 3 x {re, im}.
+int ref_incident_at(int slab, double z, double *out) {
+  C e[3];
+  incident_at(slab, z, e);
+  for (int i = 0; i < 3; ++i) {
+    out[2 * i] = e[i].real();
+    out[2 * i + 1] = e[i].imag();
+  }
+  return 0;
+}
+
+// ScatterSource::Eval (problem_common.inc:239-266), real and imaginary
+// coefficient, at reference point xi of the affine element (J row-major,
+// v0) with attribute attr: out = 3 x {re, im} of k0^2 (eps - eps_bg) Ehat.
+int ref_scatter_source(int attr, const double *J, const double *v0, const double *xi,
+                       double *out) {
+  ElementTransformation T;
+  T.Attribute = attr;
+  T.affine = true;
+  for (int i = 0; i < 9; ++i) T.J[i] = J[i];
+  for (int i = 0; i < 3; ++i) T.v0[i] = v0[i];
+  IntegrationPoint ip;
+  ip.Set3(xi[0], xi[1], xi[2]);
+  ScatterSource sre(false), sim(true);
+  Vector fr(3), fi(3);
+  sre.Eval(fr, T, ip);
+  sim.Eval(fi, T, ip);
+  for (int i = 0; i < 3; ++i) {
+    out[2 * i] = fr(i);
+    out[2 * i + 1] = fi(i);
+  }
+  return 0;
+}
+
+// ref_scatter_source over ne elements (attr[ne], J[ne*9], v0[ne*3]) at nq
+// reference points ip[nq*3]: out[(e*nq + q)*6 ...] = 3 x {re, im}.
+int ref_scatter_source_elems(int ne, const int *attr, const double *J, const double *v0,
+                             int nq, const double *ip, double *out) {
+  for (int e = 0; e < ne; ++e)
+    for (int q = 0; q < nq; ++q)
+      ref_scatter_source(attr[e], J + (size_t)e * 9, v0 + (size_t)e * 3, ip + (size_t)q * 3,
+                         out + ((size_t)e * nq + q) * 6);
   return 0;
 }
 
