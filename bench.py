@@ -222,34 +222,72 @@ def measured_peaks() -> dict:
         return {}
 
 
-def cpu_baseline_reference(case, budget_s: float, threads: int) -> dict:
+def _reference_csr(case):
+    """The reference's symbolic CSR of the mesh (build_csr_symbolic) and its
+    context, or the oracle's CSR and None without the reference build."""
+    from oracle import oracle
+    if oracle.ref_available():
+        rc = oracle.RefContext(case.ad, case.prob)
+        I, J = rc.build_csr()
+        return rc, I, J
+    I, J = oracle.csr(case.ad)
+    return None, I, J
+
+
+def cpu_baseline_reference(case, budget_s: float, threads: int, csr=None) -> dict:
     """The reference's serial CPU reassembler (reassemble_all,
     solver/asm_data.inc:374-402, compiled from its sources) on a bounded
-    element sample; with threads > 1 each thread runs it on its own sample.
-    Each sample's context and CSR are built before the timed region, one at a
-    time: the reference keeps its problem tables in a global that building a
-    context rewrites, so only the reassembly itself runs in parallel."""
+    share of the mesh: every k-th element (a mix of bulk and PML elements
+    like the whole mesh) reassembled once into the full rows of the mesh's
+    CSR, the share sized from a probe to take about ``budget_s``; nnz/s =
+    full nnz x (share elements / all elements) / wall.  With threads > 1,
+    that many disjoint strided shares run concurrently."""
     from oracle import oracle
     ne = case.ad.ne
-    kind = "reference" if oracle.ref_available() else "port"
+    if not oracle.ref_available():
+        return cpu_baseline_port(case, budget_s, threads)
+    _, I, J = csr if csr is not None else _reference_csr(case)
+    probe = oracle.RefShares(case.ad, case.prob, I, J, [np.arange(0, ne, max(1, ne // 200))])
+    t_probe = probe.time_parallel(1)
+    per_el = max(t_probe / probe.sizes[0], 1e-7)
+    del probe
+    m = int(min(ne // max(threads, 1), max(50, budget_s / per_el)))
+    stride = max(1, ne // (m * threads))
+    shares = [np.arange(k, ne, stride)[:m] for k in range(threads)]
+    sh = oracle.RefShares(case.ad, case.prob, I, J, shares)
+    wall = sh.time_parallel(threads)
+    elems = sum(sh.sizes)
+    value = len(J) * (elems / ne) / wall
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{elems} of {ne} elements (every {stride}th, {threads} thread(s) x {m}), "
+                      f"reassemble_all into the full rows of the mesh's CSR; nnz/s = full nnz x "
+                      f"sampled fraction / wall",
+            "seconds": wall}
+
+
+def cpu_baseline_port(case, budget_s: float, threads: int) -> dict:
+    """Without the reference build: the oracle (this repository's C++
+    restatement of reassemble_all) on bounded element samples, each on its
+    sample's own CSR."""
     rng = np.random.default_rng(7)
-    # calibrate on a small sample
+    ne = case.ad.ne
     probe = np.sort(rng.choice(ne, size=min(ne, 200), replace=False))
-    t_probe = _run_sample(_prepare_sample(case, probe, kind))
+    t_probe = _run_sample(_prepare_sample(case, probe, "port"))
     per_el = max(t_probe / len(probe), 1e-7)
     m = int(min(ne, max(50, budget_s / per_el / max(threads, 1))))
     samples = [np.sort(rng.choice(ne, size=m, replace=False)) for _ in range(threads)]
-    prepared = [_prepare_sample(case, smp, kind) for smp in samples]
+    prepared = [_prepare_sample(case, smp, "port") for smp in samples]
     import concurrent.futures as cf
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
         list(ex.map(_run_sample, prepared))
     wall = time.perf_counter() - t0
     elems = m * threads
-    value = case.nnz * (elems / ne) / wall
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{elems} of {ne} elements ({threads} thread(s) x {m}), reassemble_all "
-                      f"on the sample's own CSR; nnz/s = full nnz x sampled fraction / wall",
+    return {"value": case.nnz * (elems / ne) / wall, "unit": UNIT, "cores": threads,
+            "kind": "port",
+            "sample": f"{elems} of {ne} elements ({threads} thread(s) x {m}), the oracle's "
+                      f"reassembly on the sample's own CSR; nnz/s = full nnz x sampled "
+                      f"fraction / wall",
             "seconds": wall}
 
 
@@ -320,6 +358,11 @@ def main():
 
 
 def run_reference(a, rank, world, dist):
+    """The reference's CPU assembly of the whole mesh per step: its
+    reassemble_all over disjoint contiguous element shares (four per host
+    thread, handed out as threads free up) into the full rows of the mesh's
+    CSR, on every host thread; each timed step is one full pass over all
+    elements, wall clock."""
     from lithofem_b200 import configs
     from oracle import oracle
     if rank != 0:
@@ -327,37 +370,41 @@ def run_reference(a, rank, world, dist):
             dist.destroy_process_group()
         return
     case = configs.config(a.config, scale=a.scale)
-    # the reference's own symbolic CSR (build_csr_symbolic) gives nnz
-    rc = None
-    if oracle.ref_available():
-        rc = oracle.RefContext(case.ad, case.prob)
-        t0 = time.perf_counter()
-        rc.build_csr()
-        t_csr = time.perf_counter() - t0
-        case.nnz = rc.nnz
-    else:
-        case.nnz = len(oracle.csr(case.ad)[1])
-        t_csr = None
     threads = os.cpu_count() or 1
-    budget = 4.0
-    vals = []
-    info = None
-    for it in range(a.warmup + a.steps):
-        info = cpu_baseline_reference(case, budget, threads)
-        if it >= a.warmup:
-            vals.append(info["value"])
-    v = float(np.median(vals))
+    t0 = time.perf_counter()
+    rc, I, J = _reference_csr(case)
+    t_csr = time.perf_counter() - t0
+    case.nnz = len(J)
+    if rc is not None:
+        shares = oracle.contiguous_shares(case.ad.ne, 4 * threads)
+        sh = oracle.RefShares(case.ad, case.prob, I, J, shares)
+        walls = [sh.time_parallel(threads) for _ in range(a.warmup + a.steps)][a.warmup:]
+        del sh
+        kind = "reference"
+        sample = (f"all {case.ad.ne} elements every step: reassemble_all over {len(shares)} "
+                  f"contiguous element shares on {threads} threads, into the full rows of "
+                  f"the mesh's CSR (build_csr_symbolic)")
+    else:
+        walls = []
+        for _ in range(a.warmup + a.steps):
+            info = cpu_baseline_port(case, 4.0, threads)
+            walls.append(case.nnz / info["value"])
+        walls = walls[a.warmup:]
+        kind, sample = "port", info["sample"]
+    ms = 1e3 * float(np.mean(walls))
+    v = case.nnz / (ms * 1e-3)
     gpu_ref = reference_cuda_kernels(case, a, rc)
-    if gpu_ref is not None and t_csr is not None:
+    if gpu_ref is not None and rc is not None:
         gpu_ref["host_csr_build_s"] = t_csr
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 * case.nnz / v, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(case, a),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": info["kind"],
-                             "sample": info["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_wall_s": [round(w, 4) for w in walls],
             "reference_cuda_kernels": gpu_ref}
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -800,6 +847,10 @@ def cpu_baseline_batch(cases, budget_s: float, threads: int) -> dict:
 
 
 def run_reference_batch(a, rank, world, dist):
+    """The reference's CPU assembly of all 16 meshes per step, each mesh as
+    in run_reference (reassemble_all over contiguous element shares into the
+    mesh's full CSR rows, on every host thread); a step's wall time is the
+    sum over the meshes."""
     from lithofem_b200 import configs
     from oracle import oracle
     if rank != 0:
@@ -807,28 +858,40 @@ def run_reference_batch(a, rank, world, dist):
             dist.destroy_process_group()
         return
     cases = configs.batch_config(scale=a.scale)
-    for c in cases:
-        if oracle.ref_available():
-            rc = oracle.RefContext(c.ad, c.prob)
-            rc.build_csr()
-            c.nnz = rc.nnz
-        else:
-            c.nnz = len(oracle.csr(c.ad)[1])
     threads = os.cpu_count() or 1
-    vals, info = [], None
-    for it in range(a.warmup + a.steps):
-        info = cpu_baseline_batch(cases, 4.0, threads)
-        if it >= a.warmup:
-            vals.append(info["value"])
-    v = float(np.median(vals))
+    shs = []
+    for c in cases:
+        rc, I, J = _reference_csr(c)
+        c.nnz = len(J)
+        if rc is not None:
+            shs.append(oracle.RefShares(c.ad, c.prob, I, J,
+                                        oracle.contiguous_shares(c.ad.ne, 4 * threads)))
     total = sum(c.nnz for c in cases)
+    if len(shs) == len(cases):
+        walls = [sum(sh.time_parallel(threads) for sh in shs)
+                 for _ in range(a.warmup + a.steps)][a.warmup:]
+        kind = "reference"
+        sample = (f"all elements of all {len(cases)} meshes every step: reassemble_all over "
+                  f"{4 * threads} contiguous element shares per mesh on {threads} threads, "
+                  f"into each mesh's full CSR rows")
+    else:
+        walls = []
+        for _ in range(a.warmup + a.steps):
+            info = cpu_baseline_batch(cases, 4.0, threads)
+            walls.append(total / info["value"])
+        walls = walls[a.warmup:]
+        kind, sample = "port", info["sample"]
+    del shs
+    ms = 1e3 * float(np.mean(walls))
+    v = total / (ms * 1e-3)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / v,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": batch_workload_config(cases, a),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": info["kind"],
-                             "sample": info["sample"]},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_wall_s": [round(w, 4) for w in walls]}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -332,3 +332,72 @@ class RefContext:
                 self.ctx = None
         except Exception:
             pass
+
+
+def _ranges(starts: np.ndarray, lens: np.ndarray) -> np.ndarray:
+    """Concatenation of arange(s, s + l) over (starts, lens), int64."""
+    lens = np.asarray(lens, dtype=np.int64)
+    tot = int(lens.sum())
+    if tot == 0:
+        return np.zeros(0, dtype=np.int64)
+    off = np.concatenate(([0], np.cumsum(lens)[:-1]))
+    return np.repeat(np.asarray(starts, dtype=np.int64) - off, lens) + np.arange(tot, dtype=np.int64)
+
+
+def contiguous_shares(ne: int, n: int) -> list[np.ndarray]:
+    """n disjoint contiguous element ranges covering 0..ne-1."""
+    cuts = np.linspace(0, ne, n + 1).astype(np.int64)
+    return [np.arange(cuts[s], cuts[s + 1]) for s in range(n)]
+
+
+class RefShares:
+    """The reference's reassemble_all (asm_data.inc:374-402) over disjoint
+    element shares, one reference context per share.  Each share's context
+    holds the full rows of the mesh's CSR (I, J) that its elements touch, so
+    every binary search runs over a full-length row as in one serial
+    reassembly of the whole mesh; over shares that cover the mesh, the
+    shares' values summed entry by entry are the full reassembly.  All
+    contexts share the reference's global problem (set identically by each
+    context), so the shares can run on concurrent threads (ctypes releases
+    the GIL)."""
+
+    def __init__(self, ad: AsmData, prob: Problem, I: np.ndarray, J: np.ndarray,
+                 shares: list[np.ndarray]):
+        self.I, self.J = np.asarray(I), np.asarray(J)
+        self.nnz = len(J)
+        self.ctxs, self.rows, self.sizes = [], [], []
+        dof = ad.dof.reshape(ad.ne, ad.nd)
+        lens_all = np.diff(self.I.astype(np.int64))
+        for sel in shares:
+            sel = np.asarray(sel)
+            rc = RefContext(ad, prob, elements=sel)
+            rows = np.unique(dof[sel])
+            lens = np.zeros(ad.height, dtype=np.int64)
+            lens[rows] = lens_all[rows]
+            Is = np.concatenate(([0], np.cumsum(lens))).astype(np.int32)
+            Js = self.J[_ranges(self.I[rows], lens_all[rows])]
+            rc.set_csr(Is, Js)
+            self.ctxs.append(rc)
+            self.rows.append(rows)
+            self.sizes.append(len(sel))
+
+    def time_parallel(self, threads: int) -> float:
+        """Wall seconds of one reassembly of every share, `threads` at a time
+        (shares handed out as threads free up)."""
+        import concurrent.futures as cf
+        import time
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(lambda rc: rc.time_reassemble(), self.ctxs))
+        return time.perf_counter() - t0
+
+    def values(self, threads: int = 1) -> np.ndarray:
+        """The sum over the shares of their reassemblies, complex (nnz,)."""
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            parts = list(ex.map(lambda rc: rc.reassemble(), self.ctxs))
+        out = np.zeros(self.nnz, dtype=np.complex128)
+        lens_all = np.diff(self.I.astype(np.int64))
+        for rows, v in zip(self.rows, parts):
+            out[_ranges(self.I[rows], lens_all[rows])] += v   # distinct positions
+        return out
