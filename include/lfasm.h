@@ -196,10 +196,12 @@ int lfasm_residual_device(lfasm_handle *h, const void *d_x, const void *d_b,
  * framework that owns every device allocation): it allocates nothing.  Its
  * partial sums use a fixed 4 MiB device array inside the library, which
  * bounds n to 2,097,152 rows (larger n fails with LFASM_ERR_UNSUPPORTED).
- * The first call on a device looks up that array's address, so make it
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU (other streams, other host threads) race and must be
- * serialized by the caller. */
+ * Each call enqueues its two kernels and a copy of the result on `stream`,
+ * then synchronizes `stream` and returns with *rel set.  The first call on a
+ * device looks up that array's address (and looks it up again after the
+ * device's context was reset); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialized by the caller. */
 int lfasm_csr_residual_noalloc(int n, const int *d_rowptr, const int *d_cols, const void *d_vals,
                                const void *d_x, const void *d_b, double *rel, void *stream);
 
@@ -294,6 +296,16 @@ void lfasm_destroy(lfasm_handle *h);
  * -DLFASM_BOUNDS: device index checks in the gather record a failure,
  * skip the access and make the call return LFASM_ERR_CUDA), else 0. */
 int lfasm_bounds_checked(void);
+
+/* Bounds-checked debug build only (LFASM_ERR_UNSUPPORTED elsewhere; no
+ * counterpart in the reference): on device gpu_id, every bounded mbarrier
+ * wait of the warp-specialised PML kernel gives up after wait_limit
+ * try-wait rounds (<= 0: the default 2^20), and drop_first != 0 withholds
+ * the producers' arrivals on the first chunk barrier of block 0, so that the
+ * consumers' first wait there runs out: lfasm_assemble then returns
+ * LFASM_ERR_CUDA ("a bounded wait ran out") with the device still usable.
+ * Exercises the failure path without a GPU fault. */
+int lfasm_debug_wait_test(int gpu_id, long long wait_limit, int drop_first);
 
 /* Batched assembly of several meshes on one device (the reference assembles
  * one mesh per process; no counterpart).  lfasm_batch_create takes n built

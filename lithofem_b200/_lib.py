@@ -76,6 +76,7 @@ def lib() -> ct.CDLL:
         "lfasm_destroy": (None, [H]),
         "lfasm_trim_pool": (ct.c_int, [ct.c_int]),
         "lfasm_bounds_checked": (ct.c_int, []),
+        "lfasm_debug_wait_test": (ct.c_int, [ct.c_int, ct.c_longlong, ct.c_int]),
         "lfasm_set_basis": (ct.c_int, [H, ct.c_int, c_int_p, c_double_p, c_double_p]),
         "lfasm_sample_plane": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_double, ct.c_int,
                                           ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),

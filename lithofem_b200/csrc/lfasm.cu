@@ -535,6 +535,21 @@ int lfasm_bounds_checked(void) {
 #endif
 }
 
+int lfasm_debug_wait_test(int gpu_id, long long wait_limit, int drop_first) {
+  g_err.clear();
+#ifdef LFASM_BOUNDS
+  LF_CUDA(cudaSetDevice(gpu_id));
+  const long long lim = wait_limit > 0 ? wait_limit : WS_WAIT_LIMIT;
+  const int drop = drop_first ? 1 : 0;
+  LF_CUDA(cudaMemcpyToSymbol(g_ws_wait_limit, &lim, sizeof lim));
+  LF_CUDA(cudaMemcpyToSymbol(g_ws_drop_first, &drop, sizeof drop));
+  return LFASM_OK;
+#else
+  (void)gpu_id; (void)wait_limit; (void)drop_first;
+  return fail(LFASM_ERR_UNSUPPORTED, "wait test settings exist only in the bounds-checked build");
+#endif
+}
+
 int lfasm_init(const lfasm_asm_data *ad, const lfasm_problem *prob, int gpu_id,
                lfasm_handle **out) {
   g_err.clear();
@@ -1764,18 +1779,59 @@ constexpr int NOALLOC_WPB = 8;                    // rows (warps) per block
 constexpr int NOALLOC_MAX_BLOCKS = 1 << 18;       // 262144 blocks
 static __device__ __align__(256) double g_noalloc_scratch[2 * NOALLOC_MAX_BLOCKS + 2];
 
+// The array's device address per device, with the id of the CUDA context it
+// was looked up in.  A device reset (cudaDeviceReset) destroys that context
+// and the module with it; the next call sees a new context id and looks the
+// address up again instead of handing a dead address to the kernels.
+struct NoallocSlot {
+  unsigned long long ctx_id = 0;
+  double *ptr = nullptr;
+};
 std::mutex g_noalloc_mu;
-double *g_noalloc_ptr[64] = {nullptr};
+NoallocSlot g_noalloc[64];
+
+// id of the calling thread's current context (0 if none or unknown), read
+// through driver entry points obtained from the runtime (no allocation, no
+// link against the driver library)
+unsigned long long current_ctx_id() {
+  using GetCurrent = int (*)(void **);
+  using GetId = int (*)(void *, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    resolved = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();
+  }
+  if (!get_current || !get_id) return 0;
+  void *ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 int noalloc_scratch(int dev, double **out) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (dev < 0 || dev >= 64) return fail(LFASM_ERR_UNSUPPORTED, "device ordinal %d >= 64", dev);
-  if (!g_noalloc_ptr[dev]) {
+  NoallocSlot &sl = g_noalloc[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!sl.ptr || id == 0 || id != sl.ctx_id) {
+    // set-up: with the device current, the symbol's address in this
+    // context (the lookup also makes the device's context current)
     void *ptr = nullptr;
     LF_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+    sl.ptr = static_cast<double *>(ptr);
+    sl.ctx_id = current_ctx_id();
   }
-  *out = g_noalloc_ptr[dev];
+  *out = sl.ptr;
   return LFASM_OK;
 }
 }  // namespace

@@ -1391,10 +1391,21 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
       : "memory");
   return ok != 0;
 }
+#ifdef LFASM_BOUNDS
+// Debug build only: the wait limit and a test injection that withholds the
+// stagers' arrivals on block 0's first chunk barrier, so that the consumers'
+// first wait on it must run out (set by lfasm_debug_wait_test).
+__device__ long long g_ws_wait_limit = WS_WAIT_LIMIT;
+__device__ int g_ws_drop_first = 0;
+#define WS_LIMIT g_ws_wait_limit
+#else
+#define WS_LIMIT WS_WAIT_LIMIT
+#endif
 // bounded wait for the completion of the phase with the given parity;
 // false (and *err set) if it did not complete
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int *err) {
-  for (long long it = 0; it < WS_WAIT_LIMIT; ++it)
+  const long long limit = WS_LIMIT;
+  for (long long it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   atomicExch(err, 1);
   return false;
@@ -1509,7 +1520,10 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
               pml_stage_pair<LD>(qi, pr, q0 + qi, R, nd, p, te, need_v, need_c, rule, rq, tJ,
                                  tJi, tdet, tfo, qc[q0 + qi], Xs, Yr, Yi);
             }
-            mbar_arrive(&full[b]);
+#ifdef LFASM_BOUNDS
+            if (!(g_ws_drop_first && blockIdx.x == 0 && c == 0))
+#endif
+              mbar_arrive(&full[b]);
           }
         }
       }

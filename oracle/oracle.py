@@ -401,3 +401,78 @@ class RefShares:
         for rows, v in zip(self.rows, parts):
             out[_ranges(self.I[rows], lens_all[rows])] += v   # distinct positions
         return out
+
+
+DROPIN_SO = HERE / "_ref" / "libref_dropin.so"
+_dropin = None
+
+
+def dropin_available() -> bool:
+    return DROPIN_SO.exists()
+
+
+def dropin() -> ct.CDLL:
+    """INTEGRATION.md's C++ call site compiled against the reference's types
+    (oracle/ref_shim/dropin.cu), linked to liblfasm.so."""
+    global _dropin
+    if _dropin is None:
+        L = ct.CDLL(os.fspath(DROPIN_SO))
+        d, i = c_double_p, c_int_p
+        L.dropin_set_problem.argtypes = [ct.c_double] * 8 + [ct.c_int, ct.c_int, d, i, i, d]
+        L.dropin_ctx_create.argtypes = ([ct.c_int] * 4 + [i, d, i, i, d, d, d, d] +
+                                        [ct.c_int, d, d, d, d] * 2)
+        L.dropin_ctx_create.restype = ct.c_void_p
+        L.dropin_ctx_destroy.argtypes = [ct.c_void_p]
+        L.dropin_assemble.argtypes = [ct.c_void_p, i, ct.c_int, i, ct.POINTER(ct.c_longlong),
+                                      i, i, d]
+        L.dropin_assemble.restype = ct.c_int
+        _dropin = L
+    return _dropin
+
+
+def dropin_assemble(ad: AsmData, prob: Problem):
+    """The drop-in call site on (ad, prob): the reference's Problem and
+    AsmData filled from ours, then gpu_assemble.  Returns (I, J, values)."""
+    L = dropin()
+    regs = prob.regions
+    eps, dl = _c2([r.eps for r in regs]), _c2([r.delta_eps for r in regs])
+    kind = np.array([r.kind for r in regs], dtype=np.int32)
+    slab = np.array([r.slab for r in regs], dtype=np.int32)
+    L.dropin_set_problem(prob.k0, prob.kx, prob.ky, prob.z_min, prob.z_max, prob.pml_thick,
+                         prob.pml_order, prob.pml_target, ad.p, len(regs),
+                         eps.ctypes.data_as(c_double_p), kind.ctypes.data_as(c_int_p),
+                         slab.ctypes.data_as(c_int_p), dl.ctypes.data_as(c_double_p))
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data_as(c_int_p if dt == np.int32 else c_double_p)
+
+    def rule(r):
+        return [r.nq] + [arr(x, np.float64) for x in (r.ip, r.w, r.vshape, r.curl)]
+
+    fo = ad.fo if ad.p >= 2 else np.zeros(4 * ad.ne, dtype=np.int32)
+    ctx = L.dropin_ctx_create(ad.ne, ad.nd, ad.p, ad.height, arr(ad.dof, np.int32),
+                              arr(ad.sign, np.float64), arr(fo, np.int32),
+                              arr(ad.attr, np.int32), arr(ad.J, np.float64),
+                              arr(ad.Jinv, np.float64), arr(ad.detJ, np.float64),
+                              arr(ad.v0, np.float64), *rule(ad.rule_cc), *rule(ad.rule_mass))
+    try:
+        ess = np.ascontiguousarray(ad.ess, dtype=np.int32)
+        n, nnz = ct.c_int(), ct.c_longlong()
+        rc = L.dropin_assemble(ctx, ess.ctypes.data_as(c_int_p), len(ess), ct.byref(n),
+                               ct.byref(nnz), None, None, None)
+        if rc:
+            raise RuntimeError(f"drop-in call site failed at step {rc}")
+        I = np.empty(n.value + 1, dtype=np.int32)
+        J = np.empty(nnz.value, dtype=np.int32)
+        V = np.empty(2 * nnz.value)
+        rc = L.dropin_assemble(ctx, ess.ctypes.data_as(c_int_p), len(ess), ct.byref(n),
+                               ct.byref(nnz), I.ctypes.data_as(c_int_p), J.ctypes.data_as(c_int_p),
+                               V.ctypes.data_as(c_double_p))
+        if rc:
+            raise RuntimeError(f"drop-in call site failed at step {rc}")
+        return I, J, V.view(np.complex128)
+    finally:
+        L.dropin_ctx_destroy(ctx)

@@ -42,6 +42,7 @@ class Array {
   const T &operator[](int i) const { return d_[i]; }
   void Append(const T &v) { d_.push_back(v); }
   T *GetData() { return d_.data(); }
+  const T *GetData() const { return d_.data(); }
 
  private:
   std::vector<T> d_;

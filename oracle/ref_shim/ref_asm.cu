@@ -41,18 +41,9 @@ namespace {
 #include "problem_common.inc"
 #include "asm_data.inc"
 #include "asm_gpu.inc"
+#include "ref_fill.inc"
 }  // namespace
 
-namespace {
-void fill_rule(AsmRefRule &r, int nq, int nd, const double *ip, const double *w,
-               const double *v, const double *c) {
-  r.nq = nq;
-  r.ip.assign(ip, ip + (size_t)nq * 3);
-  r.w.assign(w, w + nq);
-  r.vshape.assign(v, v + (size_t)nq * nd * 3);
-  r.curl.assign(c, c + (size_t)nq * nd * 3);
-}
-}  // namespace
 
 extern "C" {
 
@@ -60,27 +51,8 @@ int ref_set_problem(double k0, double kx, double ky, double z_min, double z_max,
                     double pml_thick, double pml_order, double pml_target, int order,
                     int n_regions, const double *eps, const int *kind, const int *slab,
                     const double *delta_eps) {
-  prob = Problem();
-  prob.k0 = k0;
-  prob.kx = kx;
-  prob.ky = ky;
-  prob.z_min = z_min;
-  prob.z_max = z_max;
-  prob.pml_thick = pml_thick;
-  prob.pml_order = pml_order;
-  prob.pml_target = pml_target;
-  prob.order = order;
-  for (int r = 0; r < n_regions; ++r) {
-    Region g;
-    g.eps = C(eps[2 * r], eps[2 * r + 1]);
-    g.slab = slab[r];
-    g.is_frustum = kind[r] == 1;
-    g.is_pml = kind[r] == 2 || kind[r] == 3;
-    g.pml_top = kind[r] == 3;
-    g.delta_eps = C(delta_eps[2 * r], delta_eps[2 * r + 1]);
-    prob.regions.push_back(g);
-  }
-  return 0;
+  return fill_problem(k0, kx, ky, z_min, z_max, pml_thick, pml_order, pml_target, order,
+                      n_regions, eps, kind, slab, delta_eps);
 }
 
 void *ref_ctx_create(int ne, int nd, int p, int height, const int *dof, const double *sign,
@@ -89,24 +61,8 @@ void *ref_ctx_create(int ne, int nd, int p, int height, const int *dof, const do
                      const double *w_cc, const double *v_cc, const double *c_cc, int nq_m,
                      const double *ip_m, const double *w_m, const double *v_m,
                      const double *c_m) {
-  AsmData *ad = new AsmData();
-  ad->ne = ne;
-  ad->nd = nd;
-  ad->p = p;
-  ad->height = height;
-  ad->has_kpar = prob.kx != 0.0 || prob.ky != 0.0;
-  const size_t nen = (size_t)ne * nd;
-  ad->dof.assign(dof, dof + nen);
-  ad->sign.assign(sign, sign + nen);
-  if (p >= 2) ad->fo.assign(fo, fo + (size_t)ne * 4);
-  ad->attr.assign(attr, attr + ne);
-  ad->J.assign(J, J + (size_t)ne * 9);
-  ad->Jinv.assign(Jinv, Jinv + (size_t)ne * 9);
-  ad->detJ.assign(detJ, detJ + ne);
-  ad->v0.assign(v0, v0 + (size_t)ne * 3);
-  fill_rule(ad->rule_cc, nq_cc, nd, ip_cc, w_cc, v_cc, c_cc);
-  fill_rule(ad->rule_mass, nq_m, nd, ip_m, w_m, v_m, c_m);
-  return ad;
+  return make_asm_data(ne, nd, p, height, dof, sign, fo, attr, J, Jinv, detJ, v0, nq_cc, ip_cc,
+                       w_cc, v_cc, c_cc, nq_m, ip_m, w_m, v_m, c_m);
 }
 
 void ref_ctx_destroy(void *ctx) { delete static_cast<AsmData *>(ctx); }

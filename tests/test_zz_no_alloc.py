@@ -60,3 +60,28 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     rc, _ = _noalloc(MAX_ROWS + 1, 0, 0, 0, 0, 0)
     assert rc == 3
     assert b"allocation-free residual limit" in _lib.lib().lfasm_last_error()
+
+
+def test_noalloc_residual_at_its_row_limit():
+    """n exactly at the limit (2,097,152 rows): the last block's partial sums
+    sit next to the result slots.  A diagonal CSR gives the closed form
+    ||d x - b|| / ||b||, checked on two calls in a row."""
+    import torch
+    n = MAX_ROWS
+    rng = np.random.default_rng(17)
+    I = torch.arange(n + 1, dtype=torch.int32, device="cuda")
+    J = torch.arange(n, dtype=torch.int32, device="cuda")
+    d = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    V = torch.from_numpy(d).cuda()
+    xd = torch.from_numpy(x).cuda()
+    for call in range(2):
+        b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        if call == 1:
+            b = d * x + 1e-3 * b          # a nearly exact right-hand side
+        want = float(np.linalg.norm(d * x - b) / np.linalg.norm(b))
+        bd = torch.from_numpy(b).cuda()
+        rc, got = _noalloc(n, I.data_ptr(), J.data_ptr(), V.data_ptr(), xd.data_ptr(),
+                           bd.data_ptr())
+        assert rc == 0, _lib.lib().lfasm_last_error()
+        assert abs(got - want) <= RTOL * want, (call, got, want)
