@@ -41,6 +41,7 @@ class AsmGpu:
         self._h = ct.c_void_p()
         self._ne = self._nd = 0
         self._m = None
+        self.gpu_id = 0
 
     # -- helpers ---------------------------------------------------------
     def _ok(self, rc: int) -> bool:
@@ -62,6 +63,7 @@ class AsmGpu:
         self.Release()
         self._m = marshal(ad, self.prob, with_csr=with_csr)
         self._ne, self._nd = ad.ne, ad.nd
+        self.gpu_id = gpu_id
         return self._ok(L.lfasm_init(ct.byref(self._m.ad), ct.byref(self._m.prob), gpu_id,
                                      ct.byref(self._h)))
 
