@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="skip the solve+grad leg (device LU, plain complex128 vs mixed)")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="run only the solve+grad leg")
+    ap.add_argument("--solve-reps", type=int, default=2)
     ap.add_argument("--pml-variant", type=int, default=-1,
                     help="force the PML kernel (0 k_pml_mma, 1 k_pml_ws at p = 3, 2 k_pml_sym); "
                          "default: autotune")
@@ -438,6 +443,13 @@ def run_ours(a, rank, world, local, dist, torch):
     torch.cuda.set_device(dev)
     case = configs.config(a.config, scale=a.scale)
     ad, prob = case.ad, case.prob
+    if a.solve_only:
+        out = run_solve(a, case, dev, torch)
+        if rank == 0:
+            print(json.dumps({"solve": out}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     stream = torch.cuda.current_stream()
     g = AsmGpuGlobal(prob)
     assert g.Init(ad, dev), "lfasm_init failed"
@@ -572,6 +584,110 @@ def run_ours(a, rank, world, local, dist, torch):
     g.Release()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _timed(torch, fn):
+    """Host wall seconds of fn() with the device synchronized on both sides."""
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, out
+
+
+def run_solve(a, case, dev, torch, g=None) -> dict:
+    """The solve+grad leg on the same mesh: the plain path (assembly, complex128
+    factorization, one solve) against the mixed-precision path (assembly,
+    complex64 factorization, FP64-refined solve to 1e-10, the adjoint seed
+    of the zeroth order on a plane above the structure, FP64-refined
+    transposed solve, the per-element eps gradient), both on the device
+    through liblfasm + liblfsolve, wall clock with device syncs; the field
+    error of the mixed solution against the plain one.  The ordering (host
+    analysis, once per mesh) is reported apart."""
+    from lithofem_b200 import incident, ndbasis
+    from lithofem_b200.asm import AsmGpuGlobal
+    from lithofem_b200.solver import C64, C128, DirectSolver
+    ad, prob = case.ad, case.prob
+    own = g is None
+    if own:
+        g = AsmGpuGlobal(prob)
+        assert g.Init(ad, dev) and g.BuildGlobal(ad.ess)
+    assert g.Assemble(True)
+    n = ad.height
+    nnz = int(g.nnz())
+    parts = [incident.planewave_parts(case.stack, case.theta, 0.0, "s", 1.0, True)]
+    b = torch.zeros(n, dtype=torch.complex128, device="cuda")
+    assert g.AssembleRHS(parts, [0], 1, True, b.data_ptr())
+    assert g.SetBasis(ndbasis.nd_element(ad.p))
+    st = case.stack
+    z_plane = st.z_max - 0.25 * (st.z_max - st.slabs[-2]) if len(st.slabs) > 2 else st.z_max * 0.9
+    s = DirectSolver(dev)
+    t_an, ok = _timed(torch, lambda: s.AnalyzeAssembly(g, ad))
+    assert ok, s.last_error
+    stats = s.Stats()
+    V = g._csr()[2]
+    x128 = torch.empty_like(b)
+    x64 = torch.empty_like(b)
+    lam = torch.empty_like(b)
+    cvec = torch.empty_like(b)
+    grad = torch.zeros(ad.ne, dtype=torch.complex128, device="cuda")
+
+    def plain():
+        assert g.Assemble(True)
+        assert s.FactorDevice(V, C128), s.last_error
+        f_ms = s.Stats()["factor_ms"]
+        assert s.Backsolve(1, b.data_ptr(), x128.data_ptr()), s.last_error
+        return f_ms
+
+    def mixed():
+        assert g.Assemble(True)
+        assert s.FactorDevice(V, C64), s.last_error
+        f_ms = s.Stats()["factor_ms"]
+        ok1, rel1, it1 = s.SolveRefined(g, 1, b.data_ptr(), x64.data_ptr(), False, 1e-10)
+        assert ok1, s.last_error
+        assert g.PlaneSeed(st.lx, st.ly, z_plane, 16, 16, 0, 0, 0, cvec.data_ptr())
+        ok2, rel2, it2 = s.SolveRefined(g, 1, cvec.data_ptr(), lam.data_ptr(), True, 1e-10)
+        assert ok2, s.last_error
+        assert g.EpsGradient(parts, x64.data_ptr(), lam.data_ptr(), grad.data_ptr())
+        return f_ms, rel1[0], it1, rel2[0], it2
+
+    reps = max(1, a.solve_reps)
+    tp, tm, fp, fm, info = [], [], [], [], None
+    for _ in range(reps):
+        t, f = _timed(torch, plain)
+        tp.append(t)
+        fp.append(f)
+    res128 = g.ResidualDevice(x128.data_ptr(), b.data_ptr())[1]
+    s.Release()            # the complex128 factors out of memory
+    s = DirectSolver(dev)
+    assert s.AnalyzeAssembly(g, ad)
+    for _ in range(reps):
+        t, info = _timed(torch, mixed)
+        tm.append(t)
+        fm.append(info[0])
+    res64 = g.ResidualDevice(x64.data_ptr(), b.data_ptr())[1]
+    err = float(torch.linalg.vector_norm(x64 - x128) / torch.linalg.vector_norm(x128))
+    s.Release()
+    if own:
+        g.Release()
+    fl = stats["factor_flops"]
+    return {
+        "workload": case.name, "ndof": n, "nnz": nnz,
+        "what": "plain: assembly + complex128 LU + solve; mixed: assembly + complex64 LU + "
+                "FP64-refined solve (1e-10) + zeroth-order adjoint seed + FP64-refined "
+                "transposed solve + per-element eps gradient",
+        "timer": "host wall clock with device synchronize on both sides, best of reps",
+        "plain_s": min(tp), "mixed_s": min(tm), "mixed_over_plain": min(tm) / min(tp),
+        "factor_c128_ms": min(fp), "factor_c64_ms": min(fm),
+        "factor_tflops_c128": fl / (min(fp) * 1e-3) / 1e12,
+        "factor_tflops_c64": fl / (min(fm) * 1e-3) / 1e12,
+        "field_rel_err_mixed_vs_plain": err, "residual_plain": res128, "residual_mixed": res64,
+        "refine": {"forward_rel": info[1], "forward_corrections": info[2],
+                   "transposed_rel": info[3], "transposed_corrections": info[4]},
+        "analysis_s": t_an,
+        "fronts": stats["n_fronts"], "max_front": stats["max_front"],
+        "factor_entries": stats["factor_entries"], "factor_flops": fl,
+        "reps": reps}
 
 
 def run_e2e(a, case, dev, torch, stream) -> dict | None:

@@ -34,6 +34,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -1038,10 +1039,18 @@ int factor_impl(lfsolve *s, const double2 *vals) {
   Plan &P = s->P;
   cudaStream_t st = s->stream;
   const int D = P.max_depth + 1;
+  // LFSOLVE_PROFILE set: per-depth device times printed after the call
+  const bool prof = std::getenv("LFSOLVE_PROFILE") != nullptr;
+  std::vector<cudaEvent_t> evs;
+  if (prof) {
+    evs.resize(2 * D);
+    for (auto &e : evs) LS_CUDA(cudaEventCreate(&e));
+  }
   T *fac = static_cast<T *>(s->d_fac);
   std::vector<T *> arena(D, nullptr);
   const T one = CT<T>::mk(1.0, 0.0), mone = CT<T>::mk(-1.0, 0.0);
   for (int d = D - 1; d >= 0; --d) {
+    if (prof) LS_CUDA(cudaEventRecord(evs[2 * d], st));
     const size_t bytes = (size_t)P.arena_size[d] * sizeof(T);
     LS_CUDA(cudaMallocAsync((void **)&arena[d], std::max<size_t>(bytes, 256), st));
     LS_CUDA(cudaMemsetAsync(arena[d], 0, bytes, st));
@@ -1104,8 +1113,28 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       k_copy_out<T><<<s->n_co[d], 256, 0, st>>>(s->d_co[d], s->d_nodes, arena[d], fac);
       LS_CUDA(cudaGetLastError());
     }
+    if (prof) LS_CUDA(cudaEventRecord(evs[2 * d + 1], st));
   }
   LS_CUDA(cudaFreeAsync(arena[0], st));
+  if (prof) {
+    LS_CUDA(cudaStreamSynchronize(st));
+    for (int d = D - 1; d >= 0; --d) {
+      float ms = 0.f;
+      LS_CUDA(cudaEventElapsedTime(&ms, evs[2 * d], evs[2 * d + 1]));
+      double fl = 0.0;
+      int mmax = 0;
+      for (int id : P.by_depth[d]) {
+        const Node &N = P.nodes[id];
+        const double k = N.k, r = N.m - N.k;
+        fl += 8.0 * (k * k * k / 3.0 + k * k * r + k * r * r);
+        mmax = std::max(mmax, N.m);
+      }
+      std::printf("lfsolve profile: depth %2d fronts %5zu max m %5d  %8.2f ms  %7.2f TFLOP/s\n", d,
+                  P.by_depth[d].size(), mmax, ms, fl / (ms * 1e-3) / 1e12);
+    }
+    std::fflush(stdout);
+    for (auto &e : evs) cudaEventDestroy(e);
+  }
   return LFSOLVE_OK;
 }
 
