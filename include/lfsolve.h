@@ -105,6 +105,11 @@ int lfsolve_get_stats(lfsolve *s, lfsolve_stats *out);
  * n - n_ess non-essential rows; node_of[i] = the front that eliminates it. */
 int lfsolve_get_ordering(lfsolve *s, int *perm, int *node_of);
 
+/* The elimination tree (host), n_fronts entries each, fronts in preorder:
+ * parent front (-1 for the root), depth, pivots k and rows m (any pointer
+ * may be NULL). */
+int lfsolve_get_fronts(lfsolve *s, int *parent, int *depth, int *k, int *m);
+
 /* Releases the factors and the front workspace (the analysis stays). */
 int lfsolve_release_factors(lfsolve *s);
 

@@ -86,6 +86,7 @@ constexpr int SMALL_BWD = 6144;
 constexpr int SOLVE_THREADS = 256;
 constexpr int MAX_NRHS_PASS = 2;  // right-hand sides per solve pass
 constexpr int LANES = 8;          // streams (and library handles) for the fronts
+constexpr int BATCH_MIN = 128;    // depths with this many fronts use batched calls
 
 // ---------------------------------------------------------------------------
 // analysis (host)
@@ -101,6 +102,9 @@ struct Node {
   long long rel_off = 0;      // offset of its rows' positions in the parent front
   long long vec_off = 0;      // solve vector block offset (rows)
   int el0 = 0, el1 = 0;       // element range (leaves)
+  int ld = 0;                 // leading dimension of its front in the arena
+  int roff = 0;               // front row of its first update row (k, or the
+                              // padded pivot count of a batched depth)
 };
 
 struct Plan {
@@ -115,6 +119,13 @@ struct Plan {
   long long factor_entries = 0, vec_rows = 0;
   std::vector<int> r_orig;            // update rows (original indices), node blocks
   std::vector<int> rel;               // rows of each child in its parent front
+  std::vector<int> rel_fac;           // the same in the parent's (padded) front layout
+  // depths with many fronts are factored by batched calls on a uniform
+  // padded layout: kpad pivot rows (dummy identity pivots after the real
+  // ones), rpad update rows (zero rows after the real ones), stride per front
+  std::vector<char> batched;
+  std::vector<int> kpad, rpad;
+  std::vector<long long> stride;
   std::vector<int> ess;
   // assembly map per depth: CSR position -> arena offset
   std::vector<std::vector<int>> asm_src;
@@ -286,12 +297,40 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
   P.by_depth.assign(P.max_depth + 1, {});
   for (int s : P.post) P.by_depth[P.nodes[s].depth].push_back(s);
   P.arena_size.assign(P.max_depth + 1, 0);
+  P.batched.assign(P.max_depth + 1, 0);
+  P.kpad.assign(P.max_depth + 1, 0);
+  P.rpad.assign(P.max_depth + 1, 0);
+  P.stride.assign(P.max_depth + 1, 0);
+  // LFSOLVE_BATCH_MIN overrides the front count from which a depth is batched
+  int batch_min = BATCH_MIN;
+  if (const char *e = std::getenv("LFSOLVE_BATCH_MIN")) batch_min = std::max(1, std::atoi(e));
+  for (int d = 0; d <= P.max_depth; ++d) {
+    if ((int)P.by_depth[d].size() < batch_min) continue;
+    int kp = 0, rp = 0;
+    for (int s : P.by_depth[d]) {
+      kp = std::max(kp, P.nodes[s].k);
+      rp = std::max(rp, P.nodes[s].m - P.nodes[s].k);
+    }
+    if (kp == 0) continue;
+    P.batched[d] = 1;
+    P.kpad[d] = kp;
+    P.rpad[d] = rp;
+    P.stride[d] = align_up((long long)(kp + rp) * (kp + rp));
+  }
   long long fac = 0, roff = 0, vec = 0;
   for (int d = 0; d <= P.max_depth; ++d)
     for (int s : P.by_depth[d]) {
       Node &N = P.nodes[s];
       N.arena_off = P.arena_size[d];
-      P.arena_size[d] += align_up((long long)N.m * N.m);
+      if (P.batched[d]) {
+        N.ld = P.kpad[d] + P.rpad[d];
+        N.roff = P.kpad[d];
+        P.arena_size[d] += P.stride[d];
+      } else {
+        N.ld = N.m;
+        N.roff = N.k;
+        P.arena_size[d] += align_up((long long)N.m * N.m);
+      }
       N.fac_off = fac;
       const long long r = (long long)N.R.size();
       fac += align_up((long long)N.m * N.k + (long long)N.k * r);
@@ -313,6 +352,7 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
   // each child's update rows located in its parent's front
   std::vector<int> loc(P.nn, -1);
   P.rel.assign(roff, 0);
+  P.rel_fac.assign(roff, 0);
   for (int s = 0; s < ns; ++s) {
     const Node &N = P.nodes[s];
     if (N.nchild == 0) continue;
@@ -325,6 +365,7 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
         const int l = loc[C.R[t]];
         if (l < 0) return fail(LFSOLVE_ERR_ARG, "internal: child row missing from its parent front");
         P.rel[C.r_off + t] = l;
+        P.rel_fac[C.r_off + t] = l < N.k ? l : N.roff + (l - N.k);
       }
     }
     for (int t = 0; t < N.k; ++t) loc[N.p0 + t] = -1;
@@ -349,7 +390,7 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
   for (int s = 0; s < ns; ++s) {
     const Node &N = P.nodes[s];
     for (int t = 0; t < N.k; ++t) loc[N.p0 + t] = t;
-    for (size_t t = 0; t < N.R.size(); ++t) loc[N.R[t]] = N.k + (int)t;
+    for (size_t t = 0; t < N.R.size(); ++t) loc[N.R[t]] = N.roff + (int)t;
     auto &src = P.asm_src[N.depth];
     auto &dst = P.asm_dst[N.depth];
     for (int t = 0; t < N.k; ++t) {
@@ -361,10 +402,10 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
         const long long lj = loc[vj];
         if (lj < 0) return fail(LFSOLVE_ERR_ARG, "internal: coupling outside the front");
         src.push_back((int)p);
-        dst.push_back(N.arena_off + li + lj * N.m);
+        dst.push_back(N.arena_off + li + lj * N.ld);
         if (vj >= N.p0 + N.k) {
           src.push_back(P.tpos[p]);
-          dst.push_back(N.arena_off + lj + li * N.m);
+          dst.push_back(N.arena_off + lj + li * N.ld);
         }
       }
     }
@@ -415,7 +456,7 @@ __global__ void k_assemble(long long cnt, const int *__restrict__ src,
 struct EaItem { int child, col0; };
 struct NodeDev {  // per-node data the kernels read
   long long arena_off, fac_off, r_off, vec_off;
-  int parent, k, m, p0, depth;
+  int parent, k, m, p0, depth, ld, roff;
 };
 template <typename T>
 __global__ void k_extend_add(const EaItem *__restrict__ items, const NodeDev *__restrict__ nodes,
@@ -425,13 +466,13 @@ __global__ void k_extend_add(const EaItem *__restrict__ items, const NodeDev *__
   const NodeDev C = nodes[it.child];
   const NodeDev Pn = nodes[C.parent];
   const int r = C.m - C.k;
-  const T *U = child_arena + C.arena_off + C.k + (long long)C.k * C.m;  // F22 of the child
+  const T *U = child_arena + C.arena_off + C.roff + (long long)C.roff * C.ld;  // child's F22
   T *F = arena + Pn.arena_off;
-  const int *rl = rel + C.r_off;
+  const int *rl = rel + C.r_off;  // child rows in the parent's front layout
   const int c1 = min(it.col0 + 32, r);
   for (int b = it.col0; b < c1; ++b) {
-    const long long cb = (long long)rl[b] * Pn.m;
-    const T *Ub = U + (long long)b * C.m;
+    const long long cb = (long long)rl[b] * Pn.ld;
+    const T *Ub = U + (long long)b * C.ld;
     for (int a = threadIdx.x; a < r; a += blockDim.x) {
       T *f = F + rl[a] + cb;
       *f = cadd(*f, Ub[a]);
@@ -451,13 +492,92 @@ __global__ void k_copy_out(const EaItem *__restrict__ items, const NodeDev *__re
   T *U12 = Pf + (long long)N.m * N.k;
   const int c1 = min(it.col0 + 32, N.m);
   for (int c = it.col0; c < c1; ++c) {
-    const T *Fc = F + (long long)c * N.m;
+    // compact column c: a pivot column (< k) or update column c - k, which
+    // sits at front column roff + c - k
+    const int fc = c < N.k ? c : N.roff + (c - N.k);
+    const T *Fc = F + (long long)fc * N.ld;
     if (c < N.k) {
       T *dst = Pf + (long long)c * N.m;
-      for (int a = threadIdx.x; a < N.m; a += blockDim.x) dst[a] = Fc[a];
+      for (int a = threadIdx.x; a < N.m; a += blockDim.x)
+        dst[a] = Fc[a < N.k ? a : N.roff + (a - N.k)];
     } else {
       T *dst = U12 + (long long)(c - N.k) * N.k;
       for (int a = threadIdx.x; a < N.k; a += blockDim.x) dst[a] = Fc[a];
+    }
+  }
+}
+
+// the row interchanges of a front's pivot block (ipiv, 1-based, applied in
+// order) on ncol columns of ld-strided storage: a thread per column
+template <typename T>
+__global__ void k_swap_cols(int k, int ncol, const int *__restrict__ ipiv, T *__restrict__ A,
+                            int ld) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  T *col = A + (long long)c * ld;
+  for (int i = 0; i < k; ++i) {
+    const int p = ipiv[i] - 1;
+    if (p != i) {
+      const T t = col[i];
+      col[i] = col[p];
+      col[p] = t;
+    }
+  }
+}
+
+// batched depths: dummy identity pivots of each front (rows / columns
+// k .. kpad-1), one block per front of the depth (list in arena order)
+template <typename T>
+__global__ void k_dummy_diag(const int *__restrict__ list, const NodeDev *__restrict__ nodes,
+                             int kpad, T *__restrict__ arena) {
+  const NodeDev N = nodes[list[blockIdx.x]];
+  T *F = arena + N.arena_off;
+  for (int i = N.k + threadIdx.x; i < kpad; i += blockDim.x)
+    F[i + (long long)i * N.ld] = CT<T>::mk(1.0, 0.0);
+}
+
+// pointer arrays of a batched depth: F11, F12 and F21 of front i
+template <typename T>
+__global__ void k_make_ptrs(int cnt, T *arena, long long stride, int kpad, int ld, T **p11,
+                            T **p12, T **p21) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  T *F = arena + (long long)i * stride;
+  p11[i] = F;
+  p12[i] = F + (long long)kpad * ld;
+  p21[i] = F + kpad;
+}
+
+// the real part of the batched pivots / infos to the per-node arrays
+__global__ void k_take_pivots(const int *__restrict__ list, const NodeDev *__restrict__ nodes,
+                              int kpad, const int *__restrict__ piv, const int *__restrict__ inf,
+                              int *__restrict__ ipiv, int *__restrict__ info) {
+  const int i = blockIdx.x;
+  const int id = list[i];
+  const NodeDev N = nodes[id];
+  for (int t = threadIdx.x; t < N.k; t += blockDim.x) ipiv[N.p0 + t] = piv[(long long)i * kpad + t];
+  if (threadIdx.x == 0) info[id] = inf[i];
+}
+
+// batched depths: the fronts' row interchanges on their update columns,
+// item = (front, first of 32 columns)
+template <typename T>
+__global__ void k_swap_cols_batched(const EaItem *__restrict__ items,
+                                    const NodeDev *__restrict__ nodes,
+                                    const int *__restrict__ ipiv, T *__restrict__ arena) {
+  const EaItem it = items[blockIdx.x];
+  const NodeDev N = nodes[it.child];
+  const int r = N.m - N.k;
+  const int c = it.col0 + threadIdx.x;
+  if (threadIdx.x >= 32 || c >= r) return;
+  T *col = arena + N.arena_off + (long long)(N.roff + c) * N.ld;
+  const int *pv = ipiv + N.p0;
+  for (int i = 0; i < N.k; ++i) {
+    const int q = pv[i] - 1;
+    if (q != i) {
+      const T t = col[i];
+      col[i] = col[q];
+      col[q] = t;
     }
   }
 }
@@ -879,6 +999,42 @@ inline cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperati
   return cublasZgemm(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc);
 }
 
+inline cublasStatus_t getrf_batched(cublasHandle_t h, int n, cuComplex *const A[], int lda, int *piv,
+                                   int *info, int b) {
+  return cublasCgetrfBatched(h, n, A, lda, piv, info, b);
+}
+inline cublasStatus_t getrf_batched(cublasHandle_t h, int n, cuDoubleComplex *const A[], int lda,
+                                   int *piv, int *info, int b) {
+  return cublasZgetrfBatched(h, n, A, lda, piv, info, b);
+}
+inline cublasStatus_t trsm_batched(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t ul,
+                                   cublasOperation_t tr, cublasDiagType_t dg, int m, int n,
+                                   const cuComplex *al, const cuComplex *const A[], int lda,
+                                   cuComplex *const B[], int ldb, int b) {
+  return cublasCtrsmBatched(h, sd, ul, tr, dg, m, n, al, A, lda, B, ldb, b);
+}
+inline cublasStatus_t trsm_batched(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t ul,
+                                   cublasOperation_t tr, cublasDiagType_t dg, int m, int n,
+                                   const cuDoubleComplex *al, const cuDoubleComplex *const A[],
+                                   int lda, cuDoubleComplex *const B[], int ldb, int b) {
+  return cublasZtrsmBatched(h, sd, ul, tr, dg, m, n, al, A, lda, B, ldb, b);
+}
+inline cublasStatus_t gemm_sb(cublasHandle_t h, int m, int n, int k, const cuComplex *al,
+                              const cuComplex *A, int lda, long long sa, const cuComplex *B, int ldb,
+                              long long sb, const cuComplex *be, cuComplex *C, int ldc, long long sc,
+                              int b) {
+  return cublasCgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, al, A, lda, sa, B, ldb,
+                                   sb, be, C, ldc, sc, b);
+}
+inline cublasStatus_t gemm_sb(cublasHandle_t h, int m, int n, int k, const cuDoubleComplex *al,
+                              const cuDoubleComplex *A, int lda, long long sa,
+                              const cuDoubleComplex *B, int ldb, long long sb,
+                              const cuDoubleComplex *be, cuDoubleComplex *C, int ldc, long long sc,
+                              int b) {
+  return cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, al, A, lda, sa, B, ldb,
+                                   sb, be, C, ldc, sc, b);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -899,6 +1055,11 @@ struct lfsolve {
   std::vector<EaItem *> d_ea[2], d_co;    // per depth: extend-add items per slot, copy-out items
   std::vector<int> n_ea[2], n_co;
   std::vector<int *> d_small, d_all;      // per depth: small fronts, all fronts
+  int *d_rel_fac = nullptr;               // child rows in the parents' front layout
+  std::vector<EaItem *> d_sw;             // batched depths: swap items (front, columns)
+  std::vector<int> n_sw;
+  void **d_ptrs = nullptr;                // batched pointer arrays (3 x max fronts)
+  int *d_bpiv = nullptr, *d_binf = nullptr;
   std::vector<std::vector<int>> big;      // per depth: big fronts (host ids)
   std::vector<int> n_small;
   // factors
@@ -912,6 +1073,10 @@ struct lfsolve {
   void *work[LANES] = {};
   size_t work_bytes[LANES] = {};
   cudaEvent_t ev_main = nullptr, ev_lane[LANES] = {};
+  // the front workspace comes from a private pool that keeps its memory
+  // between depths and factorizations (a pool that hands memory back to the
+  // driver at every synchronize re-maps gigabytes per depth)
+  cudaMemPool_t pool = nullptr;
   cublasHandle_t blas_main = nullptr;
   // solve scratch
   void *d_V = nullptr, *d_bw = nullptr, *d_xr = nullptr;
@@ -944,7 +1109,8 @@ int ensure_uploaded(lfsolve *s) {
   std::vector<int> child(2 * ns, -1);
   for (int i = 0; i < ns; ++i) {
     const Node &N = P.nodes[i];
-    nd[i] = {N.arena_off, N.fac_off, N.r_off, N.vec_off, N.parent, N.k, N.m, N.p0, N.depth};
+    nd[i] = {N.arena_off, N.fac_off, N.r_off, N.vec_off, N.parent, N.k, N.m, N.p0, N.depth,
+             N.ld, N.roff};
     child[2 * i] = N.child[0];
     child[2 * i + 1] = N.nchild > 1 ? N.child[1] : -1;
   }
@@ -953,6 +1119,7 @@ int ensure_uploaded(lfsolve *s) {
   if ((rc = upload(&s->d_nodes, nd, st))) return rc;
   if ((rc = upload(&s->d_child, child, st))) return rc;
   if ((rc = upload(&s->d_rel, P.rel, st))) return rc;
+  if ((rc = upload(&s->d_rel_fac, P.rel_fac, st))) return rc;
   if ((rc = upload(&s->d_perm, P.perm, st))) return rc;
   if ((rc = upload(&s->d_rorig, P.r_orig, st))) return rc;
   if ((rc = upload(&s->d_ess, P.ess, st))) return rc;
@@ -967,6 +1134,17 @@ int ensure_uploaded(lfsolve *s) {
   s->d_all.assign(D, nullptr);
   s->n_small.assign(D, 0);
   s->big.assign(D, {});
+  s->d_sw.assign(D, nullptr);
+  s->n_sw.assign(D, 0);
+  long long maxb = 1, maxpiv = 1;
+  for (int d = 0; d < D; ++d)
+    if (P.batched[d]) {
+      maxb = std::max<long long>(maxb, (long long)P.by_depth[d].size());
+      maxpiv = std::max<long long>(maxpiv, (long long)P.by_depth[d].size() * P.kpad[d]);
+    }
+  LS_CUDA(cudaMalloc((void **)&s->d_ptrs, sizeof(void *) * 3 * maxb));
+  LS_CUDA(cudaMalloc((void **)&s->d_bpiv, sizeof(int) * maxpiv));
+  LS_CUDA(cudaMalloc((void **)&s->d_binf, sizeof(int) * maxb));
   for (int d = 0; d < D; ++d) {
     if ((rc = upload(&s->d_asm_src[d], P.asm_src[d], st))) return rc;
     if ((rc = upload(&s->d_asm_dst[d], P.asm_dst[d], st))) return rc;
@@ -986,6 +1164,15 @@ int ensure_uploaded(lfsolve *s) {
     for (int q = 0; q < 2; ++q) {
       if ((rc = upload(&s->d_ea[q][d], ea[q], st))) return rc;
       s->n_ea[q][d] = (int)ea[q].size();
+    }
+    if (P.batched[d]) {
+      std::vector<EaItem> sw;
+      for (int id : P.by_depth[d]) {
+        const Node &N = P.nodes[id];
+        for (int c0 = 0; c0 < N.m - N.k; c0 += 32) sw.push_back({id, c0});
+      }
+      if ((rc = upload(&s->d_sw[d], sw, st))) return rc;
+      s->n_sw[d] = (int)sw.size();
     }
     if ((rc = upload(&s->d_co[d], co, st))) return rc;
     s->n_co[d] = (int)co.size();
@@ -1011,6 +1198,13 @@ int ensure_lanes(lfsolve *s) {
     LS_CUDA(cudaEventCreateWithFlags(&s->ev_lane[l], cudaEventDisableTiming));
   }
   LS_CUDA(cudaEventCreateWithFlags(&s->ev_main, cudaEventDisableTiming));
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = s->dev;
+  LS_CUDA(cudaMemPoolCreate(&s->pool, &props));
+  unsigned long long keep = ~0ull;
+  LS_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   LS_CUDA(cudaEventCreate(&s->t0));
   LS_CUDA(cudaEventCreate(&s->t1));
   return LFSOLVE_OK;
@@ -1052,7 +1246,7 @@ int factor_impl(lfsolve *s, const double2 *vals) {
   for (int d = D - 1; d >= 0; --d) {
     if (prof) LS_CUDA(cudaEventRecord(evs[2 * d], st));
     const size_t bytes = (size_t)P.arena_size[d] * sizeof(T);
-    LS_CUDA(cudaMallocAsync((void **)&arena[d], std::max<size_t>(bytes, 256), st));
+    LS_CUDA(cudaMallocFromPoolAsync((void **)&arena[d], std::max<size_t>(bytes, 256), s->pool, st));
     LS_CUDA(cudaMemsetAsync(arena[d], 0, bytes, st));
     const long long na = (long long)P.asm_src[d].size();
     if (na > 0) {
@@ -1063,12 +1257,48 @@ int factor_impl(lfsolve *s, const double2 *vals) {
     if (d + 1 < D) {
       for (int q = 0; q < 2; ++q)
         if (s->n_ea[q][d] > 0) {
-          k_extend_add<T><<<s->n_ea[q][d], 256, 0, st>>>(s->d_ea[q][d], s->d_nodes, s->d_rel,
+          k_extend_add<T><<<s->n_ea[q][d], 256, 0, st>>>(s->d_ea[q][d], s->d_nodes, s->d_rel_fac,
                                                          arena[d + 1], arena[d]);
           LS_CUDA(cudaGetLastError());
         }
       LS_CUDA(cudaFreeAsync(arena[d + 1], st));
       arena[d + 1] = nullptr;
+    }
+    if (P.batched[d]) {
+      // the whole depth at once on the uniform padded layout
+      const int cnt = (int)P.by_depth[d].size();
+      const int kp = P.kpad[d], rp = P.rpad[d], ld = kp + rp;
+      const long long S = P.stride[d];
+      k_dummy_diag<T><<<cnt, 128, 0, st>>>(s->d_all[d], s->d_nodes, kp, arena[d]);
+      LS_CUDA(cudaGetLastError());
+      T **p11 = reinterpret_cast<T **>(s->d_ptrs);
+      T **p12 = p11 + cnt, **p21 = p12 + cnt;
+      k_make_ptrs<T><<<(cnt + 127) / 128, 128, 0, st>>>(cnt, arena[d], S, kp, ld, p11, p12, p21);
+      LS_CUDA(cudaGetLastError());
+      LS_BLAS(getrf_batched(s->blas_main, kp, p11, ld, s->d_bpiv, s->d_binf, cnt));
+      k_take_pivots<<<cnt, 128, 0, st>>>(s->d_all[d], s->d_nodes, kp, s->d_bpiv, s->d_binf,
+                                         s->d_ipiv, s->d_info);
+      LS_CUDA(cudaGetLastError());
+      if (rp > 0) {
+        if (s->n_sw[d] > 0) {
+          k_swap_cols_batched<T><<<s->n_sw[d], 32, 0, st>>>(s->d_sw[d], s->d_nodes, s->d_ipiv,
+                                                            arena[d]);
+          LS_CUDA(cudaGetLastError());
+        }
+        LS_BLAS(trsm_batched(s->blas_main, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                             CUBLAS_DIAG_UNIT, kp, rp, &one, p11, ld, p12, ld, cnt));
+        LS_BLAS(trsm_batched(s->blas_main, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                             CUBLAS_DIAG_NON_UNIT, rp, kp, &one, p11, ld, p21, ld, cnt));
+        LS_BLAS(gemm_sb(s->blas_main, rp, rp, kp, &mone, arena[d] + kp, ld, S,
+                        arena[d] + (long long)kp * ld, ld, S, &one,
+                        arena[d] + kp + (long long)kp * ld, ld, S, cnt));
+      }
+      if (s->n_co[d] > 0) {
+        k_copy_out<T><<<s->n_co[d], 256, 0, st>>>(s->d_co[d], s->d_nodes, arena[d], fac);
+        LS_CUDA(cudaGetLastError());
+      }
+      if (prof) LS_CUDA(cudaEventRecord(evs[2 * d + 1], st));
+      continue;
     }
     // workspace for the largest front of the depth
     int lw_max = 0;
@@ -1076,7 +1306,7 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       const Node &N = P.nodes[id];
       if (N.k == 0) continue;
       int lw = 0;
-      LS_BLAS(getrf_buf(s->sol[0], N.k, N.m, arena[d] + N.arena_off, N.m, &lw));
+      LS_BLAS(getrf_buf(s->sol[0], N.k, N.k, arena[d] + N.arena_off, N.m, &lw));
       lw_max = std::max(lw_max, lw);
     }
     for (int l = 0; l < LANES; ++l)
@@ -1099,9 +1329,16 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       const int l = li++ % LANES;
       T *F = arena[d] + N.arena_off;
       const int m = N.m, k = N.k, r = m - k;
-      LS_BLAS(getrf(s->sol[l], k, m, F, m, static_cast<T *>(s->work[l]), s->d_ipiv + N.p0,
+      // P F11 = L11 U11 (library getrf on the k x k block, swaps applied
+      // across its columns), then the same swaps on F12, U12 = L11^-1 P F12
+      LS_BLAS(getrf(s->sol[l], k, k, F, m, static_cast<T *>(s->work[l]), s->d_ipiv + N.p0,
                     s->d_info + id));
       if (r > 0) {
+        k_swap_cols<T><<<(r + 127) / 128, 128, 0, s->lane[l]>>>(k, r, s->d_ipiv + N.p0,
+                                                                F + (long long)k * m, m);
+        LS_CUDA(cudaGetLastError());
+        LS_BLAS(trsm(s->blas[l], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                     CUBLAS_DIAG_UNIT, k, r, &one, F, m, F + (long long)k * m, m));
         LS_BLAS(trsm(s->blas[l], CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
                      CUBLAS_DIAG_NON_UNIT, r, k, &one, F, m, F + k, m));
         LS_BLAS(gemm(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, r, r, k, &mone, F + k, m,
@@ -1386,6 +1623,18 @@ int lfsolve_get_ordering(lfsolve *s, int *perm, int *node_of) {
   return LFSOLVE_OK;
 }
 
+int lfsolve_get_fronts(lfsolve *s, int *parent, int *depth, int *k, int *m) {
+  if (!s || !s->analyzed) return fail(LFSOLVE_ERR_STATE, "lfsolve_analyze has not run");
+  const std::vector<Node> &nodes = s->P.nodes;
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    if (parent) parent[i] = nodes[i].parent;
+    if (depth) depth[i] = nodes[i].depth;
+    if (k) k[i] = nodes[i].k;
+    if (m) m[i] = nodes[i].m;
+  }
+  return LFSOLVE_OK;
+}
+
 int lfsolve_get_stats(lfsolve *s, lfsolve_stats *out) {
   if (!s || !out) return fail(LFSOLVE_ERR_ARG, "NULL argument");
   *out = s->st;
@@ -1522,6 +1771,10 @@ int lfsolve_release_factors(lfsolve *s) {
   if (!s) return fail(LFSOLVE_ERR_ARG, "NULL solver");
   cudaSetDevice(s->dev);
   free_factors(s);
+  if (s->pool) {
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    cudaMemPoolTrimTo(s->pool, 0);
+  }
   return LFSOLVE_OK;
 }
 
@@ -1539,6 +1792,11 @@ void lfsolve_destroy(lfsolve *s) {
   for (int q = 0; q < 2; ++q) for (auto *p : s->d_ea[q]) if (p) cudaFree(p);
   for (auto *p : s->d_co) if (p) cudaFree(p);
   for (auto *p : s->d_small) if (p) cudaFree(p);
+  for (auto *p : s->d_sw) if (p) cudaFree(p);
+  if (s->d_rel_fac) cudaFree(s->d_rel_fac);
+  if (s->d_ptrs) cudaFree(s->d_ptrs);
+  if (s->d_bpiv) cudaFree(s->d_bpiv);
+  if (s->d_binf) cudaFree(s->d_binf);
   for (auto *p : s->d_all) if (p) cudaFree(p);
   for (int l = 0; l < LANES; ++l) {
     if (s->work[l]) cudaFree(s->work[l]);
@@ -1548,6 +1806,7 @@ void lfsolve_destroy(lfsolve *s) {
     if (s->ev_lane[l]) cudaEventDestroy(s->ev_lane[l]);
   }
   if (s->blas_main) cublasDestroy(s->blas_main);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   if (s->ev_main) cudaEventDestroy(s->ev_main);
   if (s->t0) cudaEventDestroy(s->t0);
   if (s->t1) cudaEventDestroy(s->t1);

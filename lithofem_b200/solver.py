@@ -59,6 +59,7 @@ def lib() -> ct.CDLL:
                                              ct.c_int, D, I]),
         "lfsolve_get_stats": (ct.c_int, [P, ct.POINTER(Stats)]),
         "lfsolve_get_ordering": (ct.c_int, [P, I, I]),
+        "lfsolve_get_fronts": (ct.c_int, [P, I, I, I, I]),
         "lfsolve_release_factors": (ct.c_int, [P]),
         "lfsolve_destroy": (None, [P]),
     }
@@ -181,6 +182,14 @@ class DirectSolver:
         node = np.empty(nn, dtype=np.int32)
         self._check(lib().lfsolve_get_ordering(self._s, _ip(perm), _ip(node)))
         return perm, node
+
+    def Fronts(self) -> dict:
+        """The elimination tree: parent, depth, pivots k and rows m per front."""
+        nf = self.Stats()["n_fronts"]
+        out = {key: np.empty(nf, dtype=np.int32) for key in ("parent", "depth", "k", "m")}
+        self._check(lib().lfsolve_get_fronts(self._s, *[_ip(out[key]) for key in
+                                                         ("parent", "depth", "k", "m")]))
+        return out
 
     def Release(self) -> None:
         if self._s:
