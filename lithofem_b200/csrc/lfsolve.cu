@@ -1080,6 +1080,7 @@ struct lfsolve {
   cublasHandle_t blas_main = nullptr;
   // solve scratch
   void *d_V = nullptr, *d_bw = nullptr, *d_xr = nullptr;
+  size_t xr_lane = 0;  // entries of one lane's x_R scratch
   size_t V_bytes = 0, bw_bytes = 0, xr_bytes = 0;
   double2 *d_r = nullptr, *d_x64 = nullptr;
   size_t r_bytes = 0;
@@ -1389,8 +1390,16 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
   const long long VR = P.vec_rows;
   const T one = CT<T>::mk(1.0, 0.0), mone = CT<T>::mk(-1.0, 0.0);
   const int n = P.n;
+  // LFSOLVE_PROFILE set: per-depth device times of both sweeps
+  const bool prof = std::getenv("LFSOLVE_PROFILE") != nullptr;
+  std::vector<cudaEvent_t> evs;
+  if (prof) {
+    evs.resize(4 * D);
+    for (auto &e : evs) LS_CUDA(cudaEventCreate(&e));
+  }
   // forward, deepest level first
   for (int d = D - 1; d >= 0; --d) {
+    if (prof) LS_CUDA(cudaEventRecord(evs[4 * d], st));
     const int cnt = (int)P.by_depth[d].size();
     k_gather_rhs<T><<<cnt, 256, 0, st>>>(s->d_all[d], s->d_nodes, s->d_child, s->d_rel,
                                          s->d_perm, b, n, V, VR, nr);
@@ -1411,29 +1420,40 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
       }
       LS_CUDA(cudaGetLastError());
     }
-    for (int id : s->big[d]) {
-      const Node &N = P.nodes[id];
-      const int m = N.m, k = N.k, r = m - k;
-      if (k == 0) continue;  // the gathered block is its update already
-      T *v = V + N.vec_off;
-      const T *Pf = fac + N.fac_off;
-      const T *U12 = Pf + (long long)m * k;
-      if (!trans) {
-        k_laswp<T, 0><<<1, 32, 0, st>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
-        LS_CUDA(cudaGetLastError());
-        LS_BLAS(trsm(s->blas_main, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                     CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
-        if (r > 0)
-          LS_BLAS(gemm(s->blas_main, CUBLAS_OP_N, CUBLAS_OP_N, r, nr, k, &mone, Pf + k, m, v,
-                       (int)VR, &one, v + k, (int)VR));
-      } else {
-        LS_BLAS(trsm(s->blas_main, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
-                     CUBLAS_DIAG_NON_UNIT, k, nr, &one, Pf, m, v, (int)VR));
-        if (r > 0)
-          LS_BLAS(gemm(s->blas_main, CUBLAS_OP_T, CUBLAS_OP_N, r, nr, k, &mone, U12, k, v,
-                       (int)VR, &one, v + k, (int)VR));
+    // large fronts: library calls, the fronts of the depth spread over the
+    // lanes (independent vector blocks)
+    if (!s->big[d].empty()) {
+      int rc = fork_lanes(s);
+      if (rc) return rc;
+      int li = 0;
+      for (int id : s->big[d]) {
+        const Node &N = P.nodes[id];
+        const int m = N.m, k = N.k, r = m - k;
+        if (k == 0) continue;  // the gathered block is its update already
+        const int l = li++ % LANES;
+        cublasHandle_t bh = s->blas[l];
+        T *v = V + N.vec_off;
+        const T *Pf = fac + N.fac_off;
+        const T *U12 = Pf + (long long)m * k;
+        if (!trans) {
+          k_laswp<T, 0><<<1, 32, 0, s->lane[l]>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
+          LS_CUDA(cudaGetLastError());
+          LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
+          if (r > 0)
+            LS_BLAS(gemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, r, nr, k, &mone, Pf + k, m, v, (int)VR,
+                         &one, v + k, (int)VR));
+        } else {
+          LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
+                       CUBLAS_DIAG_NON_UNIT, k, nr, &one, Pf, m, v, (int)VR));
+          if (r > 0)
+            LS_BLAS(gemm(bh, CUBLAS_OP_T, CUBLAS_OP_N, r, nr, k, &mone, U12, k, v, (int)VR,
+                         &one, v + k, (int)VR));
+        }
       }
+      if ((rc = join_lanes(s))) return rc;
     }
+    if (prof) LS_CUDA(cudaEventRecord(evs[4 * d + 1], st));
   }
   // essential rows
   if (P.n_ess > 0) {
@@ -1442,6 +1462,7 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
   }
   // backward, root first
   for (int d = 0; d < D; ++d) {
+    if (prof) LS_CUDA(cudaEventRecord(evs[4 * d + 2], st));
     if (s->n_small[d] > 0) {
       int need = 0;  // rows of the largest (2 k + r) shared block
       for (int id : P.by_depth[d]) {
@@ -1460,36 +1481,59 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
       }
       LS_CUDA(cudaGetLastError());
     }
-    for (int id : s->big[d]) {
-      const Node &N = P.nodes[id];
-      const int m = N.m, k = N.k, r = m - k;
-      if (k == 0) continue;
-      T *v = V + N.vec_off;
-      const T *Pf = fac + N.fac_off;
-      const T *U12 = Pf + (long long)m * k;
-      T *xr = static_cast<T *>(s->d_xr);
-      if (r > 0) {
-        k_gather_rows<T><<<grid_for(r, 256), 256, 0, st>>>(r, s->d_rorig + N.r_off, x, n, xr, nr);
+    if (!s->big[d].empty()) {
+      int rc = fork_lanes(s);
+      if (rc) return rc;
+      int li = 0;
+      for (int id : s->big[d]) {
+        const Node &N = P.nodes[id];
+        const int m = N.m, k = N.k, r = m - k;
+        if (k == 0) continue;
+        const int l = li++ % LANES;
+        cublasHandle_t bh = s->blas[l];
+        cudaStream_t ls = s->lane[l];
+        T *v = V + N.vec_off;
+        const T *Pf = fac + N.fac_off;
+        const T *U12 = Pf + (long long)m * k;
+        T *xr = static_cast<T *>(s->d_xr) + (size_t)l * s->xr_lane;  // this lane's scratch
+        if (r > 0) {
+          k_gather_rows<T><<<grid_for(r, 256), 256, 0, ls>>>(r, s->d_rorig + N.r_off, x, n, xr, nr);
+          LS_CUDA(cudaGetLastError());
+        }
+        if (!trans) {
+          if (r > 0)
+            LS_BLAS(gemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, k, nr, r, &mone, U12, k, xr, r, &one, v,
+                         (int)VR));
+          LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_NON_UNIT, k, nr, &one, Pf, m, v, (int)VR));
+        } else {
+          if (r > 0)
+            LS_BLAS(gemm(bh, CUBLAS_OP_T, CUBLAS_OP_N, k, nr, r, &mone, Pf + k, m, xr, r, &one, v,
+                         (int)VR));
+          LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                       CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
+          k_laswp<T, 1><<<1, 32, 0, ls>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
+          LS_CUDA(cudaGetLastError());
+        }
+        k_scatter_pivots<T><<<grid_for(k, 256), 256, 0, ls>>>(k, s->d_perm + N.p0, v, VR, x, n, nr);
         LS_CUDA(cudaGetLastError());
       }
-      if (!trans) {
-        if (r > 0)
-          LS_BLAS(gemm(s->blas_main, CUBLAS_OP_N, CUBLAS_OP_N, k, nr, r, &mone, U12, k, xr, r,
-                       &one, v, (int)VR));
-        LS_BLAS(trsm(s->blas_main, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                     CUBLAS_DIAG_NON_UNIT, k, nr, &one, Pf, m, v, (int)VR));
-      } else {
-        if (r > 0)
-          LS_BLAS(gemm(s->blas_main, CUBLAS_OP_T, CUBLAS_OP_N, k, nr, r, &mone, Pf + k, m, xr, r,
-                       &one, v, (int)VR));
-        LS_BLAS(trsm(s->blas_main, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
-                     CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
-        k_laswp<T, 1><<<1, 32, 0, st>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
-        LS_CUDA(cudaGetLastError());
-      }
-      k_scatter_pivots<T><<<grid_for(k, 256), 256, 0, st>>>(k, s->d_perm + N.p0, v, VR, x, n, nr);
-      LS_CUDA(cudaGetLastError());
+      if ((rc = join_lanes(s))) return rc;
     }
+    if (prof) LS_CUDA(cudaEventRecord(evs[4 * d + 3], st));
+  }
+  if (prof) {
+    LS_CUDA(cudaStreamSynchronize(st));
+    for (int d = D - 1; d >= 0; --d) {
+      float f = 0.f, b = 0.f;
+      LS_CUDA(cudaEventElapsedTime(&f, evs[4 * d], evs[4 * d + 1]));
+      LS_CUDA(cudaEventElapsedTime(&b, evs[4 * d + 2], evs[4 * d + 3]));
+      std::printf("lfsolve solve profile (%s, %d rhs): depth %2d fronts %5zu (%zu large)  "
+                  "forward %7.3f ms  backward %7.3f ms\n", trans ? "A^T" : "A", nr, d,
+                  P.by_depth[d].size(), s->big[d].size(), f, b);
+    }
+    std::fflush(stdout);
+    for (auto &e : evs) cudaEventDestroy(e);
   }
   return LFSOLVE_OK;
 }
@@ -1504,7 +1548,8 @@ int ensure_solve_scratch(lfsolve *s, size_t es) {
   }
   size_t rmax = 1;
   for (const Node &N : P.nodes) rmax = std::max(rmax, (size_t)(N.m - N.k));
-  const size_t xr = rmax * MAX_NRHS_PASS * es;
+  s->xr_lane = rmax * MAX_NRHS_PASS;
+  const size_t xr = s->xr_lane * LANES * es;
   if (s->xr_bytes < xr) {
     if (s->d_xr) LS_CUDA(cudaFree(s->d_xr));
     LS_CUDA(cudaMalloc(&s->d_xr, xr));
