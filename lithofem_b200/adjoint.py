@@ -11,11 +11,13 @@ Gradient (A, b holomorphic in eps_e):  with A^T lambda = c,
     dJ/dRe eps_e = 2 Re(conj(l) dl/deps_e),  dJ/dIm eps_e = -2 Im(conj(l) dl/deps_e).
 
 The sparse solves are delegated to a solver object with ``solve(b)`` and
-``solve_transposed(c)``; ``HostLU`` is a stand-in for the cuDSS factorisation
-the reference uses (not present in this image): it factors the device CSR
-once on the host with SuperLU and reuses the factors for the transposed
-solve.  The assembly, right-hand side and gradient contraction run on the
-GPU (liblfasm).
+``solve_transposed(c)``.  The default is the device solver
+(``solver.DeviceLU``: liblfsolve's complex64 factorization of the device
+CSR, FP64-refined solves, the transposed solve with the same factors), the
+role cuDSS has in the reference; the ordering is computed once per mesh and
+reused by every design iteration.  ``HostLU`` (SuperLU on the host) is kept
+as a CPU cross-check.  The assembly, right-hand side and gradient
+contraction run on the GPU (liblfasm).
 """
 
 from __future__ import annotations
@@ -26,12 +28,13 @@ import numpy as np
 
 from . import ndbasis, space
 from .asm import AsmGpuGlobal
+from .solver import C64, DeviceLU, DirectSolver
 
 
 class HostLU:
-    """SuperLU factorisation of the device CSR (stand-in for cuDSS)."""
+    """SuperLU factorisation of the device CSR on the host (CPU cross-check)."""
 
-    def __init__(self, g: AsmGpuGlobal):
+    def __init__(self, g: AsmGpuGlobal, ad=None):
         import scipy.sparse as sp
         import scipy.sparse.linalg as spl
         I, J = g.DownloadCsr()
@@ -44,6 +47,25 @@ class HostLU:
 
     def solve_transposed(self, c: np.ndarray) -> np.ndarray:
         return self.lu.solve(c, trans="T")
+
+
+class _Solvers:
+    """Builds the solver for one assembled system: ``"device"`` (DeviceLU,
+    the mesh's ordering computed once and reused) or a class taking (g, ad)
+    such as HostLU."""
+
+    def __init__(self, kind, gpu_id: int, prec: int, tol: float):
+        self.kind, self.gpu_id, self.prec, self.tol = kind, gpu_id, prec, tol
+        self.analysis = None
+
+    def __call__(self, g: AsmGpuGlobal, ad):
+        if self.kind != "device":
+            return self.kind(g, ad)
+        if self.analysis is None:
+            self.analysis = DirectSolver(self.gpu_id)
+            if not self.analysis.AnalyzeAssembly(g, ad):
+                raise RuntimeError(f"lfsolve_analyze: {self.analysis.last_error}")
+        return DeviceLU(g, prec=self.prec, tol=self.tol, analysis=self.analysis)
 
 
 def plane_functional(ad: space.AsmData, z: float, lx: float, ly: float, comp: int,
@@ -81,9 +103,11 @@ def plane_functional(ad: space.AsmData, z: float, lx: float, ly: float, comp: in
 class EpsAdjoint:
     """Assemble, solve and differentiate J = |c^T u|^2 w.r.t. per-element eps."""
 
-    def __init__(self, ad, prob, parts, c: np.ndarray, gpu_id: int = 0, solver=HostLU):
+    def __init__(self, ad, prob, parts, c: np.ndarray, gpu_id: int = 0, solver="device",
+                 prec: int = C64, tol: float = 1e-12):
         self.ad, self.prob0, self.parts, self.c = ad, prob, parts, c
-        self.gpu_id, self.solver_cls = gpu_id, solver
+        self.gpu_id = gpu_id
+        self.solver_cls = _Solvers(solver, gpu_id, prec, tol)
 
     def _assemble(self, eps: np.ndarray):
         import torch
@@ -97,14 +121,14 @@ class EpsAdjoint:
 
     def value(self, eps: np.ndarray) -> complex:
         g, b = self._assemble(eps)
-        u = self.solver_cls(g).solve(b.cpu().numpy())
+        u = self.solver_cls(g, self.ad).solve(b.cpu().numpy())
         return complex(self.c @ u)
 
     def value_and_grad(self, eps: np.ndarray):
         """(l, J, dJ/dRe eps, dJ/dIm eps, dl/deps) for eps (ne complex)."""
         import torch
         g, b = self._assemble(eps)
-        lu = self.solver_cls(g)
+        lu = self.solver_cls(g, self.ad)
         u = lu.solve(b.cpu().numpy())
         lam = lu.solve_transposed(self.c)
         ell = complex(self.c @ u)
@@ -135,10 +159,13 @@ class EffAdjoint:
     """
 
     def __init__(self, ad, prob, parts, z_plane: float, lx: float, ly: float, nx: int = 8,
-                 ny: int = 8, gpu_id: int = 0, solver=HostLU):
+                 ny: int = 8, gpu_id: int = 0, solver="device", prec: int = C64,
+                 tol: float = 1e-12):
         self.ad, self.prob0, self.parts = ad, prob, parts
         self.z, self.lx, self.ly, self.nx, self.ny = z_plane, lx, ly, nx, ny
-        self.gpu_id, self.solver_cls = gpu_id, solver
+        self.gpu_id = gpu_id
+        self.solver_cls = _Solvers(solver, gpu_id, prec, tol)
+        self.last = None     # (handle, solver, u) of the last value_and_grad
         k0 = prob.k0
         kx, ky = prob.kx, prob.ky
         # top-slab incident tables of every part (one plane wave's s/p parts
@@ -189,18 +216,25 @@ class EffAdjoint:
 
     def value(self, eps) -> float:
         g, b = self._assemble(eps)
-        u = self.solver_cls(g).solve(b.cpu().numpy())
+        u = self.solver_cls(g, self.ad).solve(b.cpu().numpy())
         return self.efficiency(self.coefficient(u))
+
+    def kappa(self) -> float:
+        """eta = kappa c^H Q c."""
+        return 0.5 * self.area / (self.k0 * self.inc_flux)
+
+    def Q(self) -> np.ndarray:
+        return self._Q()
 
     def value_and_grad(self, eps):
         """(eta, deta/dRe eps, deta/dIm eps) for eps (ne complex)."""
         import torch
         g, b = self._assemble(eps)
-        lu = self.solver_cls(g)
+        lu = self.solver_cls(g, self.ad)
         u = lu.solve(b.cpu().numpy())
         c = self.coefficient(u)
         eta = self.efficiency(c)
-        kappa = 0.5 * self.area / (self.k0 * self.inc_flux)
+        kappa = self.kappa()
         gw = kappa * (self._Q() @ c)
         lam = lu.solve_transposed(np.conj(gw) @ self._seeds)
         dev = b.device
@@ -209,6 +243,7 @@ class EffAdjoint:
         gd = torch.zeros(self.ad.ne, dtype=torch.complex128, device=dev)
         assert g.EpsGradient(self.parts, ud.data_ptr(), ld.data_ptr(), gd.data_ptr())
         dl = gd.cpu().numpy()
+        self.last = (g, lu, u)
         return eta, 2.0 * np.real(dl), -2.0 * np.imag(dl)
 
 

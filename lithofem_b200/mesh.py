@@ -87,10 +87,15 @@ class Stack:
 
     @property
     def slabs(self) -> list[float]:
-        """z breakpoints of the background stack (domain bounds + layer faces)."""
+        """z breakpoints of the stack: the domain bounds, layer faces and
+        frustum base / top planes inside the domain, as the reference's
+        z_breakpoints (src/lithofem/geometry.py:221-244), so that every
+        frustum spans whole slabs."""
         zs = {self.z_min, self.z_max}
         for z0, z1, _ in self.layers:
             zs.update((z0, z1))
+        for f in self.frustums:
+            zs.update((f.z_lo, f.z_hi))
         return sorted(z for z in zs if self.z_min <= z <= self.z_max)
 
     def eps_bg_of_slab(self, i: int) -> complex:
