@@ -1,4 +1,6 @@
-"""Assembly throughput benchmark (assembled CSR nonzeros per second).
+"""Assembly throughput benchmark (assembled CSR nonzeros per second), and the
+solve+grad leg of the same metric (mixed-precision solve and adjoint
+gradient against the plain FP64 assembly + solve, in the "solve" object).
 
 One step = one pass of the system-assembly hot path over the workload:
 element matrices (curl-curl, mass and k-parallel terms with the PML
@@ -507,6 +509,12 @@ def run_ours(a, rank, world, local, dist, torch):
     # memory) + build_global + assemble + download of the CSR values
     e2e = run_e2e(a, case, dev, torch, stream)
 
+    # the metric's second half on one GPU: solve+grad, mixed vs plain FP64
+    solve = None
+    if not a.no_solve and world == 1:
+        assert g.SetAsync(False)
+        solve = run_solve(a, case, dev, torch, g)
+
     if rank != 0:
         g.Release()
         if dist is not None:
@@ -575,7 +583,8 @@ def run_ours(a, rank, world, local, dist, torch):
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "roofline": roof, "cpu_baseline": cpu, "kernels": kern, "fp64_peak_tflops": fp64,
+            "roofline": roof, "cpu_baseline": cpu, "solve": solve, "kernels": kern,
+            "fp64_peak_tflops": fp64,
             "tuning": {"bulk_variant": BULK_KERNELS[tuning[0]],
                        "bulk_ms": tuning[1],
                        "pml_variant": PML_KERNELS[pml_tuning[0]],
