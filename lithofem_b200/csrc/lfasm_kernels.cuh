@@ -1731,6 +1731,130 @@ __global__ void k_gather(int n, const int *__restrict__ long_rows, const int *__
     for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
 }
 
+// ---------------------------------------------------------------------------
+// Chunked assembly: the bulk elements are taken in chunks of consecutive
+// centroid height, and the CSR rows whose last element lies in a chunk are
+// gathered right after that chunk, while its element rows are still in L2.  Each
+// element row is read by exactly one CSR row, so after reading it the warp
+// discards its 128-byte lines from L2 (discard.global.L2: the lines are
+// dropped without being written back), and the element buffer does not have
+// to travel to DRAM and back.
+// ---------------------------------------------------------------------------
+// centroid heights of the elements of a list (sort keys) and the list
+__global__ void k_list_zkey(int n, const int *__restrict__ list, const double *__restrict__ J9,
+                            const double *__restrict__ v0, double *__restrict__ key,
+                            int *__restrict__ ids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = list[i];
+  const double *Jz = J9 + (size_t)e * 9 + 6;
+  key[i] = v0[(size_t)e * 3 + 2] + 0.25 * (Jz[0] + Jz[1] + Jz[2]);
+  ids[i] = e;
+}
+
+__global__ void k_fill_int(int n, int v, int *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+// chunk of each element from its rank in the height order
+__global__ void k_chunk_of(int ne, const int *__restrict__ sorted, int per_chunk,
+                           int *__restrict__ chunk_of) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ne) chunk_of[sorted[i]] = i / per_chunk;
+}
+
+// completion chunk of each CSR row (the last chunk holding one of its
+// element rows) and the identity permutation of the rows
+__global__ void k_row_chunk(int n, const int *__restrict__ ea_ptr, const int *__restrict__ ea,
+                            int nd, const int *__restrict__ chunk_of, int *__restrict__ comp,
+                            int *__restrict__ ids) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int c = 0;
+  for (int pp = ea_ptr[r]; pp < ea_ptr[r + 1]; ++pp) c = max(c, chunk_of[ea[pp] / nd]);
+  comp[r] = c;
+  ids[r] = r;
+}
+
+__device__ __forceinline__ void discard_l2_line(const void *p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+// Gather of the rows rows[0..n) (rows longer than maxrow are left to the
+// long-row launch), signed element rows as lfasm_assemble writes them, each
+// element row's lines discarded from L2 once the warp has added it.
+// rs is a multiple of 8: an element row is rs / 8 whole 128-byte lines.
+__global__ void k_gather_list(int n, const int *__restrict__ rows, const int *__restrict__ ea_ptr,
+                              const int *__restrict__ ea, const uint16_t *__restrict__ off,
+                              const int *__restrict__ I, const int *__restrict__ Jc,
+                              const dcplx *__restrict__ Ae, int nd, int rs,
+                              const unsigned char *__restrict__ ess, int eliminate, int maxrow,
+                              long long n_erows, dcplx *__restrict__ vals) {
+  extern __shared__ dcplx sacc[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (w >= n) return;
+  const int r = rows[w];
+  const int rb = I[r], nr = I[r + 1] - rb;
+  if (nr > maxrow) return;
+  dcplx *acc = sacc + (size_t)wib * maxrow;
+  for (int j = lane; j < nr; j += 32) acc[j] = mk(0.0, 0.0);
+  __syncwarp();
+  const int p0 = ea_ptr[r], p1 = ea_ptr[r + 1];
+  const int lines = rs >> 3;
+  if (nd <= 16) {
+    const int epi = 32 / nd;
+    const int sub = lane / nd, b = lane - sub * nd;
+    for (int q0 = p0; q0 < p1; q0 += epi) {
+      const int pp = q0 + sub;
+      dcplx v = mk(0.0, 0.0);
+      int j = -1, id = -1;
+      if (sub < epi && pp < p1) {
+        id = ea[pp];
+        if (LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) {
+          v = Ae[(size_t)id * rs + b];
+          j = off[(size_t)pp * nd + b];
+          if (!LF_CHECK(j < nr, BOUNDS_SLOT)) j = -1;
+        } else {
+          id = -1;
+        }
+      }
+      for (int t = 0; t < epi; ++t) {
+        if (sub == t && j >= 0) { acc[j].re += v.re; acc[j].im += v.im; }
+        __syncwarp();
+      }
+      if (id >= 0 && b < lines) discard_l2_line(Ae + (size_t)id * rs + 8 * b);
+    }
+  } else {
+    for (int pp = p0; pp < p1; ++pp) {
+      const int id = ea[pp];
+      if (!LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) continue;
+      const dcplx *src = Ae + (size_t)id * rs;
+      const uint16_t *o = off + (size_t)pp * nd;
+      for (int b = lane; b < nd; b += 32) {
+        const dcplx v = src[b];
+        const int j = o[b];
+        if (!LF_CHECK(j < nr, BOUNDS_SLOT)) continue;
+        acc[j].re += v.re;
+        acc[j].im += v.im;
+      }
+      __syncwarp();  // every lane's loads of this element row are consumed
+      if (lane < lines) discard_l2_line(src + 8 * lane);
+    }
+  }
+  if (eliminate && ess[r] && lane == 0) {
+    int lo = 0, hi = nr - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (Jc[rb + mid] < r) lo = mid + 1; else hi = mid;
+    }
+    acc[lo] = mk(1.0, 0.0);
+  }
+  __syncwarp();
+  for (int j = lane; j < nr; j += 32) vals[rb + j] = acc[j];
+}
+
 // rows longer than cap, in any order
 __global__ void k_long_rows(int n, const int *__restrict__ I, int cap, int *__restrict__ out,
                             int *__restrict__ count) {

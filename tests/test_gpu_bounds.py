@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 ROOT = Path(__file__).resolve().parents[1]
 
 SCRIPT = r"""
-import sys, numpy as np
+import os, sys, numpy as np
 sys.path.insert(0, %(root)r)
 from lithofem_b200 import _lib, configs
 from lithofem_b200.asm import AsmGpuGlobal
@@ -34,6 +34,15 @@ for c in cases:
         ref = oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, elim)
         r = np.abs(g.DownloadValues() - ref).max() / np.abs(ref).max()
         assert r < 1e-13, r
+# the chunked assembly (many chunks) under the same checks
+os.environ["LFASM_CHUNK_MB"] = "0.05"
+c = configs.small_case("grating", 3, 6.0, seed=13, h=3.2)
+g = AsmGpuGlobal(c.prob)
+assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess)
+I, J = oracle.csr(c.ad)
+assert g.Assemble(True), g.last_error
+ref = oracle.assemble(c.ad, c.prob, I, J, c.ad.ess, True)
+assert np.abs(g.DownloadValues() - ref).max() / np.abs(ref).max() < 1e-13
 print("bounds build ok")
 """
 
@@ -47,7 +56,7 @@ def test_bounds_checked_build_on_parity_cases():
 
 
 WAIT_SCRIPT = r"""
-import sys, numpy as np
+import os, sys, numpy as np
 sys.path.insert(0, %(root)r)
 from lithofem_b200 import _lib, configs
 from lithofem_b200.asm import AsmGpuGlobal
