@@ -77,6 +77,11 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr long long ALIGN = 32;  // front / factor block alignment (entries)
 inline long long align_up(long long x) { return (x + ALIGN - 1) / ALIGN * ALIGN; }
+// pivot blocks and leading dimensions of the fronts are padded to this many
+// entries, so that F11, F12, F21 and F22 all start on 128-byte boundaries
+// (256 for complex128) with row strides of whole 128-byte lines
+constexpr int FPAD = 16;
+inline int pad_up(int x) { return (x + FPAD - 1) / FPAD * FPAD; }
 
 // fronts with at most SMALL_M rows (and 2 k + r <= SMALL_BWD) are solved by
 // one block each, with the right-hand-side block in shared memory: m x nrhs
@@ -87,6 +92,9 @@ constexpr int SOLVE_THREADS = 256;
 constexpr int MAX_NRHS_PASS = 2;  // right-hand sides per solve pass
 constexpr int LANES = 8;          // streams (and library handles) for the fronts
 constexpr int BATCH_MIN = 128;    // depths with this many fronts use batched calls
+// complex64 fronts whose Schur update F22 -= L21 U12 has at least this many
+// complex multiply-adds use three TF32 tensor-core GEMMs on split operands
+constexpr double TF32X3_MIN_MACS = 2e9;
 
 // ---------------------------------------------------------------------------
 // analysis (host)
@@ -313,9 +321,10 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
     }
     if (kp == 0) continue;
     P.batched[d] = 1;
-    P.kpad[d] = kp;
-    P.rpad[d] = rp;
-    P.stride[d] = align_up((long long)(kp + rp) * (kp + rp));
+    P.kpad[d] = pad_up(kp);
+    P.rpad[d] = pad_up(P.kpad[d] + rp) - P.kpad[d];
+    const long long ld = P.kpad[d] + P.rpad[d];
+    P.stride[d] = align_up(ld * ld);
   }
   long long fac = 0, roff = 0, vec = 0;
   for (int d = 0; d <= P.max_depth; ++d)
@@ -327,9 +336,11 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
         N.roff = P.kpad[d];
         P.arena_size[d] += P.stride[d];
       } else {
-        N.ld = N.m;
-        N.roff = N.k;
-        P.arena_size[d] += align_up((long long)N.m * N.m);
+        // dummy identity pivots k .. roff-1 after the real ones, zero rows
+        // and columns past the update rows up to ld
+        N.roff = pad_up(N.k);
+        N.ld = pad_up(N.roff + (N.m - N.k));
+        P.arena_size[d] += align_up((long long)N.ld * N.ld);
       }
       N.fac_off = fac;
       const long long r = (long long)N.R.size();
@@ -525,14 +536,14 @@ __global__ void k_swap_cols(int k, int ncol, const int *__restrict__ ipiv, T *__
   }
 }
 
-// batched depths: dummy identity pivots of each front (rows / columns
-// k .. kpad-1), one block per front of the depth (list in arena order)
+// dummy identity pivots of each front (rows / columns k .. roff-1), one
+// block per front of the depth (list in arena order)
 template <typename T>
 __global__ void k_dummy_diag(const int *__restrict__ list, const NodeDev *__restrict__ nodes,
-                             int kpad, T *__restrict__ arena) {
+                             T *__restrict__ arena) {
   const NodeDev N = nodes[list[blockIdx.x]];
   T *F = arena + N.arena_off;
-  for (int i = N.k + threadIdx.x; i < kpad; i += blockDim.x)
+  for (int i = N.k + threadIdx.x; i < N.roff; i += blockDim.x)
     F[i + (long long)i * N.ld] = CT<T>::mk(1.0, 0.0);
 }
 
@@ -579,6 +590,55 @@ __global__ void k_swap_cols_batched(const EaItem *__restrict__ items,
       col[i] = col[q];
       col[q] = t;
     }
+  }
+}
+
+// Error-compensated TF32 operands of F22 -= L21 U12 (complex64, kk pivot
+// columns incl. dummies, r update rows), in a real formulation: the complex
+// product is the real product of A (2r x 2kk; column 2j is column j of L21
+// read as (re, im) float pairs, column 2j + 1 that of i L21) and B (2kk x r;
+// U12 read as (re, im) pairs), and the real result read as floats is F22
+// itself (leading dimension 2 ld).  Every float x is split as hi = its TF32
+// rounding (cvt.rna.tf32.f32, 10 mantissa bits) and lo = x - hi;
+// hi hi' + hi lo' + lo hi' carries the product to about 2^-22 relative on
+// TF32 tensor cores.  A is stored as [hi | lo] (2r x 4kk, leading dimension
+// lda), B as [lo ; hi] (4kk x r, leading dimension 4kk), so that two GEMMs
+// ([hi | lo] [lo ; hi] and hi hi) cover the three products.
+__device__ __forceinline__ float tf32_round(float x) {
+  unsigned u;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+  return __uint_as_float(u);
+}
+__device__ __forceinline__ void tf32_split(cuComplex v, float2 &h, float2 &l) {
+  h = make_float2(tf32_round(v.x), tf32_round(v.y));
+  l = make_float2(v.x - h.x, v.y - h.y);
+}
+__global__ void k_split_a(int r, int kk, const cuComplex *__restrict__ L, int ld,
+                          float *__restrict__ A, int lda) {
+  const long long n = (long long)r * kk, lo_off = (long long)2 * kk * lda;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % r), j = (int)(t / r);
+    float2 h, l;
+    tf32_split(L[i + (long long)j * ld], h, l);
+    float *c0 = A + (long long)(2 * j) * lda + 2 * i;  // column 2j; 2j + 1 one lda on
+    *reinterpret_cast<float2 *>(c0) = h;
+    *reinterpret_cast<float2 *>(c0 + lda) = make_float2(-h.y, h.x);
+    *reinterpret_cast<float2 *>(c0 + lo_off) = l;
+    *reinterpret_cast<float2 *>(c0 + lo_off + lda) = make_float2(-l.y, l.x);
+  }
+}
+__global__ void k_split_b(int kk, int r, const cuComplex *__restrict__ U, int ld,
+                          float *__restrict__ B) {
+  const long long n = (long long)kk * r;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(t % kk), c = (int)(t / kk);
+    float2 h, l;
+    tf32_split(U[j + (long long)c * ld], h, l);
+    float *col = B + (long long)c * 4 * kk;
+    *reinterpret_cast<float2 *>(col + 2 * j) = l;
+    *reinterpret_cast<float2 *>(col + 2 * kk + 2 * j) = h;
   }
 }
 
@@ -1077,6 +1137,11 @@ struct lfsolve {
   // between depths and factorizations (a pool that hands memory back to the
   // driver at every synchronize re-maps gigabytes per depth)
   cudaMemPool_t pool = nullptr;
+  // 3xTF32 Schur updates of large complex64 fronts: per-lane split buffers
+  void *split[LANES] = {};
+  size_t split_bytes[LANES] = {};
+  int *lpiv[LANES] = {};  // pivots of a front's padded pivot block
+  int lpiv_n[LANES] = {};
   cublasHandle_t blas_main = nullptr;
   // solve scratch
   void *d_V = nullptr, *d_bw = nullptr, *d_xr = nullptr;
@@ -1229,6 +1294,51 @@ int grid_for(long long n, int threads) {
   return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 16));
 }
 
+// fronts from this many complex multiply-adds of Schur update on
+// (LFSOLVE_TF32X3_MIN overrides TF32X3_MIN_MACS)
+double tf32x3_min() {
+  const char *e = std::getenv("LFSOLVE_TF32X3_MIN");
+  return e ? std::atof(e) : TF32X3_MIN_MACS;
+}
+
+// the 3xTF32 path: complex64 only, off with LFSOLVE_TF32X3=0
+template <typename T> bool use_tf32x3(lfsolve *) { return false; }
+template <> bool use_tf32x3<cuComplex>(lfsolve *) {
+  const char *e = std::getenv("LFSOLVE_TF32X3");
+  return !(e && e[0] == '0');
+}
+
+// F22 -= L21 U12 of one complex64 front (at F, leading dimension ld, kk
+// pivot rows incl. dummies, r update rows) on lane l: split both operands,
+// then the two TF32 tensor-core GEMMs of the real formulation with FP32
+// accumulation into F22
+int schur_tf32x3(lfsolve *s, int l, cuComplex *F, int ld, int kk, int r) {
+  const long long lda = ((2LL * r + 31) / 32) * 32;
+  const size_t na = (size_t)lda * 4 * kk, need = (na + (size_t)4 * kk * r) * sizeof(float);
+  if (s->split_bytes[l] < need) {
+    LS_CUDA(cudaStreamSynchronize(s->lane[l]));
+    if (s->split[l]) LS_CUDA(cudaFree(s->split[l]));
+    LS_CUDA(cudaMalloc(&s->split[l], need));
+    s->split_bytes[l] = need;
+  }
+  float *A = static_cast<float *>(s->split[l]);
+  float *B = A + na;
+  const int g = grid_for((long long)r * kk, 256);
+  k_split_a<<<g, 256, 0, s->lane[l]>>>(r, kk, F + kk, ld, A, (int)lda);
+  LS_CUDA(cudaGetLastError());
+  k_split_b<<<g, 256, 0, s->lane[l]>>>(kk, r, F + (long long)kk * ld, ld, B);
+  LS_CUDA(cudaGetLastError());
+  const float mone = -1.f, one = 1.f;
+  float *C = reinterpret_cast<float *>(F + kk + (long long)kk * ld);
+  LS_BLAS(cublasGemmEx(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, 2 * r, r, 4 * kk, &mone, A,
+                       CUDA_R_32F, (int)lda, B, CUDA_R_32F, 4 * kk, &one, C, CUDA_R_32F, 2 * ld,
+                       CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+  LS_BLAS(cublasGemmEx(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, 2 * r, r, 2 * kk, &mone, A,
+                       CUDA_R_32F, (int)lda, B + 2 * kk, CUDA_R_32F, 4 * kk, &one, C,
+                       CUDA_R_32F, 2 * ld, CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+  return LFSOLVE_OK;
+}
+
 template <typename T>
 int factor_impl(lfsolve *s, const double2 *vals) {
   Plan &P = s->P;
@@ -1270,7 +1380,7 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       const int cnt = (int)P.by_depth[d].size();
       const int kp = P.kpad[d], rp = P.rpad[d], ld = kp + rp;
       const long long S = P.stride[d];
-      k_dummy_diag<T><<<cnt, 128, 0, st>>>(s->d_all[d], s->d_nodes, kp, arena[d]);
+      k_dummy_diag<T><<<cnt, 128, 0, st>>>(s->d_all[d], s->d_nodes, arena[d]);
       LS_CUDA(cudaGetLastError());
       T **p11 = reinterpret_cast<T **>(s->d_ptrs);
       T **p12 = p11 + cnt, **p21 = p12 + cnt;
@@ -1301,22 +1411,33 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       if (prof) LS_CUDA(cudaEventRecord(evs[2 * d + 1], st));
       continue;
     }
-    // workspace for the largest front of the depth
-    int lw_max = 0;
+    // workspace and pivot scratch for the largest front of the depth
+    int lw_max = 0, kk_max = 0;
     for (int id : P.by_depth[d]) {
       const Node &N = P.nodes[id];
       if (N.k == 0) continue;
       int lw = 0;
-      LS_BLAS(getrf_buf(s->sol[0], N.k, N.k, arena[d] + N.arena_off, N.m, &lw));
+      LS_BLAS(getrf_buf(s->sol[0], N.roff, N.roff, arena[d] + N.arena_off, N.ld, &lw));
       lw_max = std::max(lw_max, lw);
+      kk_max = std::max(kk_max, N.roff);
     }
-    for (int l = 0; l < LANES; ++l)
+    for (int l = 0; l < LANES; ++l) {
       if (s->work_bytes[l] < (size_t)lw_max * sizeof(T)) {
         LS_CUDA(cudaStreamSynchronize(st));
         if (s->work[l]) LS_CUDA(cudaFree(s->work[l]));
         s->work_bytes[l] = (size_t)lw_max * sizeof(T);
         LS_CUDA(cudaMalloc(&s->work[l], s->work_bytes[l]));
       }
+      if (s->lpiv_n[l] < kk_max) {
+        LS_CUDA(cudaStreamSynchronize(st));
+        if (s->lpiv[l]) LS_CUDA(cudaFree(s->lpiv[l]));
+        s->lpiv_n[l] = kk_max;
+        LS_CUDA(cudaMalloc((void **)&s->lpiv[l], sizeof(int) * kk_max));
+      }
+    }
+    const int cnt = (int)P.by_depth[d].size();
+    k_dummy_diag<T><<<cnt, 128, 0, st>>>(s->d_all[d], s->d_nodes, arena[d]);
+    LS_CUDA(cudaGetLastError());
     int rc = fork_lanes(s);
     if (rc) return rc;
     // largest fronts first, spread over the lanes
@@ -1329,21 +1450,29 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       if (N.k == 0) continue;
       const int l = li++ % LANES;
       T *F = arena[d] + N.arena_off;
-      const int m = N.m, k = N.k, r = m - k;
-      // P F11 = L11 U11 (library getrf on the k x k block, swaps applied
-      // across its columns), then the same swaps on F12, U12 = L11^-1 P F12
-      LS_BLAS(getrf(s->sol[l], k, k, F, m, static_cast<T *>(s->work[l]), s->d_ipiv + N.p0,
+      const int k = N.k, r = N.m - N.k, kk = N.roff, ld = N.ld;
+      // P F11 = L11 U11 (library getrf on the kk x kk block: the k real
+      // pivots, then dummy identity pivots that never swap), the real swaps
+      // on F12, U12 = L11^-1 P F12, L21 = F21 U11^-1, F22 -= L21 U12
+      LS_BLAS(getrf(s->sol[l], kk, kk, F, ld, static_cast<T *>(s->work[l]), s->lpiv[l],
                     s->d_info + id));
+      LS_CUDA(cudaMemcpyAsync(s->d_ipiv + N.p0, s->lpiv[l], sizeof(int) * k,
+                              cudaMemcpyDeviceToDevice, s->lane[l]));
       if (r > 0) {
         k_swap_cols<T><<<(r + 127) / 128, 128, 0, s->lane[l]>>>(k, r, s->d_ipiv + N.p0,
-                                                                F + (long long)k * m, m);
+                                                                F + (long long)kk * ld, ld);
         LS_CUDA(cudaGetLastError());
         LS_BLAS(trsm(s->blas[l], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                     CUBLAS_DIAG_UNIT, k, r, &one, F, m, F + (long long)k * m, m));
+                     CUBLAS_DIAG_UNIT, kk, r, &one, F, ld, F + (long long)kk * ld, ld));
         LS_BLAS(trsm(s->blas[l], CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                     CUBLAS_DIAG_NON_UNIT, r, k, &one, F, m, F + k, m));
-        LS_BLAS(gemm(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, r, r, k, &mone, F + k, m,
-                     F + (long long)k * m, m, &one, F + k + (long long)k * m, m));
+                     CUBLAS_DIAG_NON_UNIT, r, kk, &one, F, ld, F + kk, ld));
+        if (use_tf32x3<T>(s) && (double)r * r * kk >= tf32x3_min()) {
+          int rc3 = schur_tf32x3(s, l, reinterpret_cast<cuComplex *>(F), ld, kk, r);
+          if (rc3) return rc3;
+        } else {
+          LS_BLAS(gemm(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, r, r, kk, &mone, F + kk, ld,
+                       F + (long long)kk * ld, ld, &one, F + kk + (long long)kk * ld, ld));
+        }
       }
     }
     if ((rc = join_lanes(s))) return rc;
@@ -1845,6 +1974,8 @@ void lfsolve_destroy(lfsolve *s) {
   for (auto *p : s->d_all) if (p) cudaFree(p);
   for (int l = 0; l < LANES; ++l) {
     if (s->work[l]) cudaFree(s->work[l]);
+    if (s->split[l]) cudaFree(s->split[l]);
+    if (s->lpiv[l]) cudaFree(s->lpiv[l]);
     if (s->blas[l]) cublasDestroy(s->blas[l]);
     if (s->sol[l]) cusolverDnDestroy(s->sol[l]);
     if (s->lane[l]) cudaStreamDestroy(s->lane[l]);
