@@ -278,6 +278,44 @@ int lfasm_sample_plane(lfasm_handle *h, double lx, double ly, double z, int nx, 
 int lfasm_plane_seed(lfasm_handle *h, double lx, double ly, double z, int nx, int ny, int comp,
                      int m, int q, void *d_c);
 
+/* Several planes and their diffraction orders on the device (the reference
+ * samples its reflection and transmission planes one after the other,
+ * solver/lithofem_solve.cpp:951-1015, then FFTs each on the host,
+ * src/lithofem/orders.py:36-67, and forms the order efficiencies of
+ * src/lithofem/outputs.py:219-269).
+ * lfasm_sample_planes: lfasm_sample_plane for nz planes at heights z[0 ..
+ * nz) (host array) in one pass; d_e / d_curl hold nz blocks of ny * nx * 3
+ * complex128 (plane-major).  At most LFASM_MAX_PLANES planes and 2^24 points.
+ * lfasm_plane_orders: for every plane iz of such samples d_e and every
+ * grid index o = b nx + a of the order (m, n) = (a or a - nx above nx / 2,
+ * b or b - ny above ny / 2): d_coef[(iz nx ny + o) 3 + c] = (1 / (nx ny))
+ * sum_{j,i} E_c(x_ij) exp(-2 pi i (a i / nx + b j / ny)) (numpy's fft2
+ * divided by nx ny), and d_eff[iz nx ny + o] the order's efficiency: with
+ * kx = args->kx + 2 pi m / lx, ky likewise, qz = sqrt(k0^2 eps - kx^2 -
+ * ky^2) (Im qz >= 0) and c' = c exp(-i d qz (z - z_ref)) plus bg00 for the
+ * (0, 0) order when has_bg00, eff = d Re[(c' x conj(k x c' / k0))_z] lx ly /
+ * (2 inc_flux), k = (kx, ky, d qz), d = direction (+1: up-going orders of a
+ * reflection plane, -1: down-going of a transmission plane). */
+#define LFASM_MAX_PLANES 256
+typedef struct {
+  double z, z_ref;       /* sampled height, reference plane of the efficiency */
+  double eps_re, eps_im; /* permittivity of the one-way region */
+  int direction;         /* +1 or -1 */
+  int has_bg00;          /* add bg00 to the (0, 0) coefficient at z_ref */
+  double bg00[6];        /* analytic (0, 0) background, 3 complex (re, im) */
+} lfasm_order_plane;
+typedef struct {
+  double lx, ly;   /* cell */
+  double k0;       /* vacuum wavenumber */
+  double kx, ky;   /* Bloch wavevector of the incidence */
+  double inc_flux; /* incident flux through the cell */
+} lfasm_order_args;
+int lfasm_sample_planes(lfasm_handle *h, double lx, double ly, int nz, const double *z, int nx,
+                        int ny, const void *d_u, void *d_e, void *d_curl);
+int lfasm_plane_orders(lfasm_handle *h, int nz, int nx, int ny, const void *d_e,
+                       const lfasm_order_plane *planes, const lfasm_order_args *args,
+                       void *d_coef, double *d_eff);
+
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
  * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the

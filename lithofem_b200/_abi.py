@@ -66,6 +66,19 @@ def _c2(z) -> np.ndarray:
     return np.ascontiguousarray(np.stack([z.real, z.imag], axis=-1).reshape(-1))
 
 
+class OrderPlaneC(ct.Structure):
+    """lfasm_order_plane: one sampled plane of lfasm_plane_orders."""
+    _fields_ = [("z", ct.c_double), ("z_ref", ct.c_double), ("eps_re", ct.c_double),
+                ("eps_im", ct.c_double), ("direction", ct.c_int), ("has_bg00", ct.c_int),
+                ("bg00", ct.c_double * 6)]
+
+
+class OrderArgsC(ct.Structure):
+    """lfasm_order_args: cell, wavenumber, Bloch wavevector, incident flux."""
+    _fields_ = [("lx", ct.c_double), ("ly", ct.c_double), ("k0", ct.c_double),
+                ("kx", ct.c_double), ("ky", ct.c_double), ("inc_flux", ct.c_double)]
+
+
 @dataclass
 class Marshalled:
     """C structs plus the numpy buffers that keep their pointers alive."""

@@ -10,7 +10,8 @@ import ctypes as ct
 import os
 from pathlib import Path
 
-from ._abi import AsmDataC, IncidentPartC, ProblemC, c_double_p, c_int_p
+from ._abi import (AsmDataC, IncidentPartC, OrderArgsC, OrderPlaneC, ProblemC, c_double_p,
+                   c_int_p)
 
 LIB_PATH = Path(__file__).resolve().parent / "liblfasm.so"
 # LFASM_LIBRARY selects another build of the same library (the
@@ -82,6 +83,12 @@ def lib() -> ct.CDLL:
                                           ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
         "lfasm_plane_seed": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_double, ct.c_int,
                                         ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p]),
+        "lfasm_sample_planes": (ct.c_int, [H, ct.c_double, ct.c_double, ct.c_int, c_double_p,
+                                           ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p,
+                                           ct.c_void_p]),
+        "lfasm_plane_orders": (ct.c_int, [H, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p,
+                                          ct.POINTER(OrderPlaneC), ct.POINTER(OrderArgsC),
+                                          ct.c_void_p, ct.c_void_p]),
         "lfasm_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
         "lfasm_batch_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
         "lfasm_batch_assemble": (ct.c_int, [ct.c_void_p, ct.c_int]),

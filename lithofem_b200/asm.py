@@ -16,7 +16,7 @@ import ctypes as ct
 
 import numpy as np
 
-from . import _lib
+from . import _abi, _lib
 from ._abi import (BULK_VARIANTS, CROSS0, CROSS1, CURLCURL, KLK, MASS, c_double_p, c_int_p, marshal,
                    marshal_parts)
 from .problem import Problem
@@ -137,6 +137,40 @@ class AsmGpu:
         return self._ok(_lib.lib().lfasm_sample_plane(
             self._h, float(lx), float(ly), float(z), int(nx), int(ny), ct.c_void_p(u_ptr),
             ct.c_void_p(e_ptr or None), ct.c_void_p(curl_ptr or None)))
+
+    def SamplePlanes(self, lx: float, ly: float, zs, nx: int, ny: int, u_ptr: int, e_ptr: int,
+                     curl_ptr: int = 0) -> bool:
+        """SamplePlane for every height of zs in one pass: [len(zs)][ny][nx][3]
+        complex128 into e_ptr / curl_ptr (device)."""
+        z = np.ascontiguousarray(zs, dtype=np.float64)
+        return self._ok(_lib.lib().lfasm_sample_planes(
+            self._h, float(lx), float(ly), len(z), z.ctypes.data_as(c_double_p), int(nx),
+            int(ny), ct.c_void_p(u_ptr), ct.c_void_p(e_ptr or None),
+            ct.c_void_p(curl_ptr or None)))
+
+    def PlaneOrders(self, nx: int, ny: int, e_ptr: int, planes, args, coef_ptr: int,
+                    eff_ptr: int) -> bool:
+        """Fourier orders (coef_ptr: [nz][ny * nx][3] complex128) and order
+        efficiencies (eff_ptr: [nz][ny * nx] float64) of sampled planes.
+        planes: sequence of dicts with z, z_ref, eps, direction and optional
+        bg00 (3 complex); args: dict with lx, ly, k0, kx, ky, inc_flux."""
+        arr = (_abi.OrderPlaneC * len(planes))()
+        for i, q in enumerate(planes):
+            eps = complex(q["eps"])
+            arr[i].z, arr[i].z_ref = float(q["z"]), float(q["z_ref"])
+            arr[i].eps_re, arr[i].eps_im = eps.real, eps.imag
+            arr[i].direction = int(q["direction"])
+            bg = q.get("bg00")
+            arr[i].has_bg00 = 0 if bg is None else 1
+            if bg is not None:
+                b = np.asarray(bg, dtype=np.complex128).reshape(3)
+                for c in range(3):
+                    arr[i].bg00[2 * c], arr[i].bg00[2 * c + 1] = b[c].real, b[c].imag
+        a = _abi.OrderArgsC(float(args["lx"]), float(args["ly"]), float(args["k0"]),
+                            float(args["kx"]), float(args["ky"]), float(args["inc_flux"]))
+        return self._ok(_lib.lib().lfasm_plane_orders(
+            self._h, len(planes), int(nx), int(ny), ct.c_void_p(e_ptr), arr, ct.byref(a),
+            ct.c_void_p(coef_ptr), ct.c_void_p(eff_ptr)))
 
     def PlaneSeed(self, lx: float, ly: float, z: float, nx: int, ny: int, comp: int, m: int,
                   q: int, c_ptr: int) -> bool:

@@ -1797,42 +1797,51 @@ namespace {
 
 // locate the nx x ny sample points of the plane z: element and reference
 // coordinates per point (device arrays owned by the caller afterwards)
-int plane_locate(lfasm_handle *h, const PlaneGrid &G, int **elem, double **xi) {
+// Sample points of nz planes (heights zs, host) located in the mesh: per
+// plane the elements whose z-range holds it (flags [iz][e], one scan, one
+// compaction), then a warp per point over its plane's candidates; *elem
+// and *xi (device, nz * nx * ny points) are the caller's to free.
+int plane_locate(lfasm_handle *h, const PlaneGrid &G, int nz, const double *zs, int **elem,
+                 double **xi) {
   const int ne = h->ne, npts = G.nx * G.ny;
+  const long long nf = (long long)ne * nz, ntot = (long long)npts * nz;
   int *flag = nullptr, *pos = nullptr, *cand = nullptr, *miss = nullptr;
+  double *dz = nullptr;
   unsigned char *tmp = nullptr;
   size_t tb = 0;
-  LF_CUDA(dmalloc(flag, (size_t)ne + 1));
-  LF_CUDA(dmalloc(pos, (size_t)ne + 1));
-  LF_CUDA(dmalloc(cand, (size_t)ne));
+  LF_CUDA(dmalloc(flag, (size_t)nf + 1));
+  LF_CUDA(dmalloc(pos, (size_t)nf + 1));
+  LF_CUDA(dmalloc(cand, (size_t)nf));
   LF_CUDA(dmalloc(miss, 1));
-  LF_CUDA(dmalloc(*elem, (size_t)npts));
-  LF_CUDA(dmalloc(*xi, (size_t)npts * 3));
-  LF_CUDA(cudaMemsetAsync(flag + ne, 0, sizeof(int), h->stream));
+  LF_CUDA(dmalloc(dz, (size_t)nz));
+  LF_CUDA(dmalloc(*elem, (size_t)ntot));
+  LF_CUDA(dmalloc(*xi, (size_t)ntot * 3));
+  LF_CUDA(cudaMemcpyAsync(dz, zs, sizeof(double) * nz, cudaMemcpyHostToDevice, h->stream));
+  LF_CUDA(cudaMemsetAsync(flag + nf, 0, sizeof(int), h->stream));
   LF_CUDA(cudaMemsetAsync(miss, 0, sizeof(int), h->stream));
-  const unsigned gb = (unsigned)((ne + 255) / 256);
-  k_plane_cand<<<gb, 256, 0, h->stream>>>(ne, h->J, h->v0, G.z - 4.9e-7, flag);
+  const unsigned gb = (unsigned)((nf + 255) / 256);
+  k_plane_cand<<<gb, 256, 0, h->stream>>>(ne, nz, h->J, h->v0, dz, flag);
   LF_LAUNCHED();
-  LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, ne + 1, h->stream));
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, (int)(nf + 1), h->stream));
   LF_CUDA(dmalloc(tmp, tb));
-  LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, pos, ne + 1, h->stream));
-  k_compact<<<gb, 256, 0, h->stream>>>(ne, flag, pos, cand);
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, pos, (int)(nf + 1), h->stream));
+  k_compact<<<gb, 256, 0, h->stream>>>((int)nf, flag, pos, cand);
   LF_LAUNCHED();
-  int ncand = 0;
-  LF_CUDA(cudaMemcpyAsync(&ncand, pos + ne, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  LF_CUDA(cudaStreamSynchronize(h->stream));
   const int wpb = 8;
-  k_plane_locate<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
-      G, ncand, cand, h->Jinv, h->v0, *elem, *xi, miss);
+  k_plane_locate<<<(unsigned)((ntot + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
+      G, nz, dz, ne, pos, cand, h->Jinv, h->v0, *elem, *xi, miss);
   LF_LAUNCHED();
   int nmiss = 0;
   LF_CUDA(cudaMemcpyAsync(&nmiss, miss, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   LF_CUDA(cudaStreamSynchronize(h->stream));
-  dfree(flag); dfree(pos); dfree(cand); dfree(miss); dfree(tmp);
+  dfree(flag); dfree(pos); dfree(cand); dfree(miss); dfree(tmp); dfree(dz);
   if (nmiss) {
     dfree(*elem); dfree(*xi);
-    return fail(LFASM_ERR_ARG, "%d of %d sample points of the plane z = %g lie outside the mesh",
-                nmiss, npts, G.z);
+    if (nz == 1)
+      return fail(LFASM_ERR_ARG, "%d of %d sample points of the plane z = %g lie outside the mesh",
+                  nmiss, npts, zs[0]);
+    return fail(LFASM_ERR_ARG, "%d of %lld sample points of the %d planes lie outside the mesh",
+                nmiss, ntot, nz);
   }
   return LFASM_OK;
 }
@@ -1860,7 +1869,7 @@ int lfasm_sample_plane(lfasm_handle *h, double lx, double ly, double z, int nx, 
   LF_CUDA(cudaSetDevice(h->dev));
   int *elem = nullptr;
   double *xi = nullptr;
-  if ((rc = plane_locate(h, G, &elem, &xi))) return rc;
+  if ((rc = plane_locate(h, G, 1, &z, &elem, &xi))) return rc;
   const int npts = nx * ny, wpb = 8;
   k_plane_eval<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
       npts, elem, xi, h->nd, h->p, h->nmono, h->bexps, h->bcoef, h->bccoef, h->dof, h->sign,
@@ -1882,7 +1891,7 @@ int lfasm_plane_seed(lfasm_handle *h, double lx, double ly, double z, int nx, in
   LF_CUDA(cudaSetDevice(h->dev));
   int *elem = nullptr;
   double *xi = nullptr;
-  if ((rc = plane_locate(h, G, &elem, &xi))) return rc;
+  if ((rc = plane_locate(h, G, 1, &z, &elem, &xi))) return rc;
   const int npts = nx * ny, wpb = 8;
   LF_CUDA(cudaMemsetAsync(d_c, 0, (size_t)h->n * sizeof(dcplx), h->stream));
   k_plane_seed<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
@@ -1891,6 +1900,89 @@ int lfasm_plane_seed(lfasm_handle *h, double lx, double ly, double z, int nx, in
   LF_LAUNCHED();
   LF_CUDA(cudaStreamSynchronize(h->stream));
   dfree(elem); dfree(xi);
+  return sync_if(h);
+}
+
+int lfasm_sample_planes(lfasm_handle *h, double lx, double ly, int nz, const double *z, int nx,
+                        int ny, const void *d_u, void *d_e, void *d_curl) {
+  PlaneGrid G;
+  int rc = plane_args(h, lx, ly, 0.0, nx, ny, G);
+  if (rc) return rc;
+  if (nz <= 0 || nz > LFASM_MAX_PLANES || !z)
+    return fail(LFASM_ERR_ARG, "bad plane list (%d planes, at most %d)", nz, LFASM_MAX_PLANES);
+  if ((long long)nx * ny * nz > (1ll << 24))
+    return fail(LFASM_ERR_ARG, "%d planes of %d x %d points exceed 2^24 points", nz, nx, ny);
+  if (!d_u || (!d_e && !d_curl)) return fail(LFASM_ERR_ARG, "NULL vector");
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(h->dev));
+  int *elem = nullptr;
+  double *xi = nullptr;
+  if ((rc = plane_locate(h, G, nz, z, &elem, &xi))) return rc;
+  const long long npts = (long long)nx * ny * nz;
+  const int wpb = 8;
+  k_plane_eval<<<(unsigned)((npts + wpb - 1) / wpb), wpb * 32, 0, h->stream>>>(
+      (int)npts, elem, xi, h->nd, h->p, h->nmono, h->bexps, h->bcoef, h->bccoef, h->dof, h->sign,
+      h->fopack, h->J, h->Jinv, h->detJ, (const dcplx *)d_u, (dcplx *)d_e, (dcplx *)d_curl);
+  LF_LAUNCHED();
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(elem); dfree(xi);
+  return sync_if(h);
+}
+
+int lfasm_plane_orders(lfasm_handle *h, int nz, int nx, int ny, const void *d_e,
+                       const lfasm_order_plane *planes, const lfasm_order_args *args,
+                       void *d_coef, double *d_eff) {
+  if (!h) return fail(LFASM_ERR_ARG, "NULL handle");
+  if (nz <= 0 || nz > LFASM_MAX_PLANES || !planes || !args)
+    return fail(LFASM_ERR_ARG, "bad plane list (%d planes, at most %d)", nz, LFASM_MAX_PLANES);
+  if (nx <= 0 || ny <= 0 || (long long)nx * ny * nz > (1ll << 24))
+    return fail(LFASM_ERR_ARG, "bad sampling grid %d x %d x %d planes", nx, ny, nz);
+  if (!d_e || !d_coef || !d_eff) return fail(LFASM_ERR_ARG, "NULL vector");
+  const lfasm_order_args &a = *args;
+  if (!(a.lx > 0) || !(a.ly > 0) || !(a.k0 > 0) || !(a.inc_flux > 0))
+    return fail(LFASM_ERR_ARG, "bad cell %g x %g, k0 %g or incident flux %g", a.lx, a.ly, a.k0,
+                a.inc_flux);
+  for (int i = 0; i < nz; ++i)
+    if (planes[i].direction != 1 && planes[i].direction != -1)
+      return fail(LFASM_ERR_ARG, "plane %d: direction %d is not +1 or -1", i,
+                  planes[i].direction);
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(h->dev));
+  // per-plane scalars packed into one upload: z, z_ref, eps (2), background (6)
+  std::vector<double> hp((size_t)nz * 10);
+  std::vector<int> hd(nz);
+  bool any_bg = false;
+  for (int i = 0; i < nz; ++i) {
+    const lfasm_order_plane &q = planes[i];
+    double *r = hp.data() + (size_t)i * 10;
+    r[0] = q.z; r[1] = q.z_ref; r[2] = q.eps_re; r[3] = q.eps_im;
+    for (int c = 0; c < 6; ++c) r[4 + c] = q.bg00[c];
+    any_bg = any_bg || q.has_bg00;
+    if (!q.has_bg00)
+      for (int c = 0; c < 6; ++c) r[4 + c] = 0.0;
+    hd[i] = q.direction;
+  }
+  double *dp = nullptr;
+  int *dd = nullptr;
+  LF_CUDA(dmalloc(dp, hp.size()));
+  LF_CUDA(dmalloc(dd, hd.size()));
+  LF_CUDA(cudaMemcpyAsync(dp, hp.data(), sizeof(double) * hp.size(), cudaMemcpyHostToDevice,
+                          h->stream));
+  LF_CUDA(cudaMemcpyAsync(dd, hd.data(), sizeof(int) * hd.size(), cudaMemcpyHostToDevice,
+                          h->stream));
+  // split the packed rows into the kernel's arrays: z, z_ref, eps, background
+  double *zs = nullptr;
+  LF_CUDA(dmalloc(zs, (size_t)nz * 10));
+  k_unpack_planes<<<(nz + 127) / 128, 128, 0, h->stream>>>(nz, dp, zs, zs + nz, zs + 2 * nz,
+                                                            zs + 4 * nz);
+  LF_LAUNCHED();
+  OrderArgs A{a.lx, a.ly, a.k0, a.kx, a.ky, a.inc_flux};
+  k_plane_orders<<<dim3((unsigned)(nx * ny), (unsigned)nz), ORDER_THREADS, 0, h->stream>>>(
+      nx, ny, (const dcplx *)d_e, zs, zs + nz, dd, zs + 2 * nz, any_bg ? zs + 4 * nz : nullptr,
+      A, (dcplx *)d_coef, d_eff);
+  LF_LAUNCHED();
+  LF_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(dp); dfree(dd); dfree(zs);
   return sync_if(h);
 }
 

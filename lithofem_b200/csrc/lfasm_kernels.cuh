@@ -2449,19 +2449,24 @@ struct PlaneGrid {
   int nx, ny;
 };
 
-// sample point (i, j): cell-centred with the reference's fixed nudges
-__device__ __forceinline__ void plane_point(const PlaneGrid &G, int pt, double x[3]) {
+// sample point (i, j) of a plane at height z: cell-centred with the
+// reference's fixed nudges
+__device__ __forceinline__ void plane_point(const PlaneGrid &G, int pt, double z, double x[3]) {
   const int i = pt % G.nx, j = pt / G.nx;
   x[0] = (i + 0.5) * G.lx / G.nx + 3.1e-7;
   x[1] = (j + 0.5) * G.ly / G.ny + 1.7e-7;
-  x[2] = G.z - 4.9e-7;
+  x[2] = z - 4.9e-7;
 }
 
-// elements whose z-range contains z (vertex z = v0z + J20 / J21 / J22)
-__global__ void k_plane_cand(int ne, const double *__restrict__ J9, const double *__restrict__ v0,
-                             double z, int *__restrict__ flag) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= ne) return;
+// elements whose z-range contains the nudged height of plane iz (vertex
+// z = v0z + J20 / J21 / J22); flags [iz][e] for nz planes
+__global__ void k_plane_cand(int ne, int nz, const double *__restrict__ J9,
+                             const double *__restrict__ v0, const double *__restrict__ zs,
+                             int *__restrict__ flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)ne * nz) return;
+  const int e = (int)(t % ne), iz = (int)(t / ne);
+  const double z = zs[iz] - 4.9e-7;
   const double z0 = v0[(size_t)e * 3 + 2];
   double lo = z0, hi = z0;
   for (int c = 0; c < 3; ++c) {
@@ -2470,7 +2475,7 @@ __global__ void k_plane_cand(int ne, const double *__restrict__ J9, const double
     hi = fmax(hi, zc);
   }
   const double tol = 1e-9 * (1.0 + fabs(z));
-  flag[e] = (z >= lo - tol && z <= hi + tol) ? 1 : 0;
+  flag[t] = (z >= lo - tol && z <= hi + tol) ? 1 : 0;
 }
 
 __global__ void k_compact(int n, const int *__restrict__ flag, const int *__restrict__ pos,
@@ -2479,23 +2484,29 @@ __global__ void k_compact(int n, const int *__restrict__ flag, const int *__rest
   if (e < n && flag[e]) out[pos[e]] = e;
 }
 
-// one warp per sample point: the candidate element in which the point is
-// most interior (largest smallest barycentric coordinate; lower index on a
-// tie) and the point's reference coordinates; *missing counts points that
-// lie outside every candidate
-__global__ void k_plane_locate(PlaneGrid G, int ncand, const int *__restrict__ cand,
+// one warp per sample point of nz planes (point pt of plane pt / (nx ny)):
+// the candidate element of its plane (cand[pos[iz ne] .. pos[(iz + 1) ne]))
+// in which the point is most interior (largest smallest barycentric
+// coordinate; lower index on a tie) and the point's reference coordinates;
+// *missing counts points that lie outside every candidate
+__global__ void k_plane_locate(PlaneGrid G, int nz, const double *__restrict__ zs, int ne,
+                               const int *__restrict__ pos, const int *__restrict__ cand,
                                const double *__restrict__ Ji9, const double *__restrict__ v0,
                                int *__restrict__ elem, double *__restrict__ xi,
                                int *__restrict__ missing) {
   const int lane = threadIdx.x & 31;
-  const int pt = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (pt >= G.nx * G.ny) return;
+  const int npts = G.nx * G.ny;
+  const long long ptg = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ptg >= (long long)npts * nz) return;
+  const int iz = (int)(ptg / npts), pt = (int)ptg;
   double x[3];
-  plane_point(G, pt, x);
+  plane_point(G, pt % npts, zs[iz], x);
   double best = -1e300;
   int be = 0x7fffffff;
-  for (int i = lane; i < ncand; i += 32) {
-    const int e = cand[i];
+  // the compaction kept flattened (plane, element) indices iz ne + e
+  const int c0 = pos[(size_t)iz * ne], c1 = pos[(size_t)(iz + 1) * ne];
+  for (int i = c0 + lane; i < c1; i += 32) {
+    const int e = cand[i] - iz * ne;
     const double *Ji = Ji9 + (size_t)e * 9;
     const double d0 = x[0] - v0[(size_t)e * 3], d1 = x[1] - v0[(size_t)e * 3 + 1],
                  d2 = x[2] - v0[(size_t)e * 3 + 2];
@@ -2657,6 +2668,116 @@ __global__ void k_plane_seed(PlaneGrid G, const int *__restrict__ elem,
     atomicAdd(dst, w * cs);
     atomicAdd(dst + 1, w * sn);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fourier orders of sampled planes and their efficiencies (the reference's
+// orders_from_plane and order efficiency, src/lithofem/orders.py:36-67 and
+// src/lithofem/outputs.py:219-269).  Block (order o, plane iz): the
+// coefficient c = (1 / (nx ny)) sum_{j,i} E(x_ij) exp(-2 pi i (a i / nx +
+// b j / ny)) of the order at grid index o = b nx + a (order m = a, or
+// a - nx above nx / 2; n likewise), its qz = sqrt(k0^2 eps - kx^2 - ky^2)
+// with Im qz >= 0, and the efficiency of the coefficient carried to the
+// reference plane, c' = c exp(-i d qz (z - z_ref)) (+ the analytic (0,0)
+// background there): d Re[(c' x conj(k x c' / k0))_z] area / (2 inc_flux),
+// k = (kx, ky, d qz), d = +1 (reflection side) or -1 (transmission side).
+// ---------------------------------------------------------------------------
+struct OrderArgs {
+  double lx, ly, k0, kx, ky, inc_flux;
+};
+constexpr int ORDER_THREADS = 128;
+
+// principal square root (Re >= 0), the half-angle formulas evaluated
+// without cancellation on either sign of the real part
+__device__ __forceinline__ dcplx csqrt_principal(dcplx w) {
+  const double r = hypot(w.re, w.im);
+  if (r == 0.0) return mk(0.0, 0.0);
+  if (w.re >= 0.0) {
+    const double t = sqrt(0.5 * (r + w.re));
+    return mk(t, w.im / (2.0 * t));
+  }
+  const double t = sqrt(0.5 * (r - w.re));
+  return mk(fabs(w.im) / (2.0 * t), copysign(t, w.im));
+}
+
+// rows of 10 (z, z_ref, eps re/im, background 3 complex) to separate arrays
+__global__ void k_unpack_planes(int nz, const double *__restrict__ rows, double *__restrict__ z,
+                                double *__restrict__ zref, double *__restrict__ eps2,
+                                double *__restrict__ bg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nz) return;
+  const double *r = rows + (size_t)i * 10;
+  z[i] = r[0];
+  zref[i] = r[1];
+  eps2[2 * i] = r[2];
+  eps2[2 * i + 1] = r[3];
+  for (int c = 0; c < 6; ++c) bg[6 * i + c] = r[4 + c];
+}
+
+__global__ void __launch_bounds__(ORDER_THREADS)
+k_plane_orders(int nx, int ny, const dcplx *__restrict__ E, const double *__restrict__ zs,
+               const double *__restrict__ zref, const int *__restrict__ dirs,
+               const double *__restrict__ eps2, const double *__restrict__ bg, OrderArgs A,
+               dcplx *__restrict__ coef, double *__restrict__ eff) {
+  const int npts = nx * ny, o = blockIdx.x, iz = blockIdx.y;
+  const int a = o % nx, b = o / nx;
+  const dcplx *Ez = E + (size_t)iz * npts * 3;
+  const long long per = (long long)nx * ny;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int pt = threadIdx.x; pt < npts; pt += ORDER_THREADS) {
+    const int i = pt % nx, j = pt / nx;
+    // phase -2 pi (a i / nx + b j / ny), reduced to one period first
+    const long long num = ((long long)a * i * ny + (long long)b * j * nx) % per;
+    double sn, cs;
+    sincospi(-2.0 * (double)num / (double)per, &sn, &cs);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const dcplx u = Ez[(size_t)pt * 3 + c];
+      s[2 * c] += u.re * cs - u.im * sn;
+      s[2 * c + 1] += u.re * sn + u.im * cs;
+    }
+  }
+  __shared__ double red[6][ORDER_THREADS];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) red[q][threadIdx.x] = s[q];
+  __syncthreads();
+  for (int w = ORDER_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x) return;
+  const double inv = 1.0 / (double)npts;
+  dcplx c[3];
+  for (int q = 0; q < 3; ++q) {
+    c[q] = mk(red[2 * q][0] * inv, red[2 * q + 1][0] * inv);
+    coef[((size_t)iz * npts + o) * 3 + q] = c[q];
+  }
+  const int m = a <= nx / 2 ? a : a - nx, n = b <= ny / 2 ? b : b - ny;
+  const double kx = A.kx + 2.0 * 3.141592653589793238 / A.lx * m;
+  const double ky = A.ky + 2.0 * 3.141592653589793238 / A.ly * n;
+  const dcplx ep = mk(eps2[2 * iz], eps2[2 * iz + 1]);
+  dcplx qz = csqrt_principal(mk(A.k0 * A.k0 * ep.re - kx * kx - ky * ky, A.k0 * A.k0 * ep.im));
+  if (qz.im < 0.0) qz = mk(-qz.re, -qz.im);
+  const int d = dirs[iz];
+  // c' = c exp(-i d qz dz) = c e^{d dz Im qz} (cos(d dz Re qz) - i sin(d dz Re qz))
+  const double dz = zs[iz] - zref[iz];
+  const double g = exp(d * dz * qz.im);
+  double sn, cs;
+  sincos(d * dz * qz.re, &sn, &cs);
+  const dcplx ph = mk(g * cs, -g * sn);
+  for (int q = 0; q < 3; ++q) {
+    c[q] = cmul(c[q], ph);
+    if (m == 0 && n == 0 && bg) c[q] = cadd(c[q], mk(bg[6 * iz + 2 * q], bg[6 * iz + 2 * q + 1]));
+  }
+  const dcplx kz = mk(d * qz.re, d * qz.im);
+  // h = k x c / k0 (x and y components)
+  const dcplx hx = cscale(1.0 / A.k0, cadd(cscale(ky, c[2]), cscale(-1.0, cmul(kz, c[1]))));
+  const dcplx hy = cscale(1.0 / A.k0, cadd(cmul(kz, c[0]), cscale(-kx, c[2])));
+  // Re[(c x conj(h))_z] = Re[c_x conj(h_y) - c_y conj(h_x)]
+  const double sz = (c[0].re * hy.re + c[0].im * hy.im) - (c[1].re * hx.re + c[1].im * hx.im);
+  eff[(size_t)iz * npts + o] = d * 0.5 * sz * A.lx * A.ly / A.inc_flux;
 }
 
 }  // namespace lfasm_dev

@@ -110,3 +110,28 @@ def order_efficiencies(oset: OrderSet, z: float, z_ref: float, direction: int, a
         out[(int(oset.ms[i]), int(oset.ns[i]))] = direction * plane_wave_flux(
             c, oset.kx[i], oset.ky[i], oset.qz[i], oset.k0, direction, area) / inc_flux
     return out
+
+
+def device_orders(g, nx: int, ny: int, e_ptr: int, planes, lx: float, ly: float, k0: float,
+                  kpar: tuple[float, float], inc_flux: float):
+    """Orders and efficiencies of nz sampled planes on the device
+    (lfasm_plane_orders over samples written by lfasm_sample_planes at
+    e_ptr).  planes: dicts with z, z_ref, eps, direction (+1 reflection,
+    -1 transmission) and optional bg00.  Returns, per plane, the
+    (ny * nx, 3) coefficients in orders_from_plane's order and the
+    efficiency of every order keyed (m, n) as order_efficiencies."""
+    import torch
+    nz = len(planes)
+    coef = torch.empty(nz * ny * nx * 3, dtype=torch.complex128, device="cuda")
+    eff = torch.empty(nz * ny * nx, dtype=torch.float64, device="cuda")
+    args = dict(lx=lx, ly=ly, k0=k0, kx=kpar[0], ky=kpar[1], inc_flux=inc_flux)
+    if not g.PlaneOrders(nx, ny, e_ptr, planes, args, coef.data_ptr(), eff.data_ptr()):
+        raise RuntimeError(f"lfasm_plane_orders failed: {g.last_error}")
+    c = coef.cpu().numpy().reshape(nz, ny * nx, 3)
+    e = eff.cpu().numpy().reshape(nz, ny * nx)
+    ms = np.array([i if i <= nx // 2 else i - nx for _ in range(ny) for i in range(nx)])
+    ns = np.array([j if j <= ny // 2 else j - ny for j in range(ny) for _ in range(nx)])
+    out = []
+    for iz in range(nz):
+        out.append((c[iz], {(int(ms[o]), int(ns[o])): float(e[iz, o]) for o in range(ny * nx)}))
+    return out
