@@ -585,6 +585,9 @@ def run_ours(a, rank, world, local, dist, torch):
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "roofline": roof, "cpu_baseline": cpu, "solve": solve, "kernels": kern,
             "fp64_peak_tflops": fp64,
+            "host_build_s": dict(case.host_s, what="host mesh generation and space / per-mesh "
+                                 "data extraction (build_asm_data) of this mesh, once per "
+                                 "mesh, outside the timed regions"),
             "tuning": {"bulk_variant": BULK_KERNELS[tuning[0]],
                        "bulk_ms": tuning[1],
                        "pml_variant": PML_KERNELS[pml_tuning[0]],

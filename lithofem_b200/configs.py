@@ -11,11 +11,12 @@ the actual element, DOF and nonzero counts are reported by the callers.
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
+import time
+from dataclasses import dataclass, field
 
 import numpy as np
 
-from .mesh import Frustum, Stack, build_mesh, h_for_target_dofs
+from .mesh import Frustum, Stack, TetMesh, build_mesh, h_for_target_dofs
 from .mesh_poly import PolyHole, build_poly_mesh, random_hole
 from .problem import Problem
 from .space import AsmData, build_asm_data
@@ -60,6 +61,11 @@ class Case:
     theta: float
     ad: AsmData
     prob: Problem
+    mesh: TetMesh | None = None
+    h: float = 0.0
+    # host seconds of the final mesh generation and of the space / per-mesh
+    # data extraction (build_asm_data)
+    host_s: dict = field(default_factory=dict)
 
     def summary(self) -> dict:
         nb = None
@@ -76,11 +82,15 @@ def make_case(name: str, stack: Stack, p: int, theta: float, ndof_target: float 
         h = h_for_target_dofs(stack, p, ndof_target)
         trial = build_asm_data(build_mesh(stack, h), p, prob)
         h *= (trial.height / ndof_target) ** (1.0 / 3.0)
+    t0 = time.perf_counter()
     mesh = build_mesh(stack, h)
+    t1 = time.perf_counter()
     ad = build_asm_data(mesh, p, prob, build_csr=build_csr, local_order_seed=local_order_seed)
+    t2 = time.perf_counter()
     if elem_eps:
         prob.elem_eps = absorber_jitter(ad, prob)
-    return Case(name=name, stack=stack, p=p, theta=theta, ad=ad, prob=prob)
+    return Case(name=name, stack=stack, p=p, theta=theta, ad=ad, prob=prob, mesh=mesh, h=h,
+                host_s={"mesh": t1 - t0, "space": t2 - t1})
 
 
 def make_poly_case(name: str, stack: Stack, p: int, theta: float,
