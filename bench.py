@@ -575,6 +575,13 @@ def run_ours(a, rank, world, local, dist, torch):
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"failed: {exc}"}
 
+    # the same extraction on the device (lfasm_extract, host copies included)
+    from lithofem_b200 import space
+    t0 = time.perf_counter()
+    space.build_asm_data_device(case.mesh, case.p, prob, gpu_id=dev)
+    extract_s = {"extract": time.perf_counter() - t0,
+                 "what": "lfasm_extract of the same mesh: mesh upload, device numbering and "
+                         "per-mesh data, download of the arrays (wall clock)"}
     cfg = workload_config(case, a)
     cfg["nnz"] = int(case.nnz)
     cfg["bulk_elements"], cfg["pml_elements"] = nb, npml
@@ -588,6 +595,7 @@ def run_ours(a, rank, world, local, dist, torch):
             "host_build_s": dict(case.host_s, what="host mesh generation and space / per-mesh "
                                  "data extraction (build_asm_data) of this mesh, once per "
                                  "mesh, outside the timed regions"),
+            "device_extract_s": extract_s,
             "tuning": {"bulk_variant": BULK_KERNELS[tuning[0]],
                        "bulk_ms": tuning[1],
                        "pml_variant": PML_KERNELS[pml_tuning[0]],

@@ -316,6 +316,23 @@ int lfasm_plane_orders(lfasm_handle *h, int nz, int nx, int ny, const void *d_e,
                        const lfasm_order_plane *planes, const lfasm_order_args *args,
                        void *d_coef, double *d_eff);
 
+/* Per-mesh data on the device (the reference's extract_asm_data over MFEM's
+ * Nedelec space, solver/asm_data.inc:99-173, run on the host there):
+ * from ne tetrahedra with topological vertex ids tv[4 e + i] (0 .. nv-1,
+ * after periodic identification) and their own vertex coordinates
+ * xv[(4 e + i) 3 + d], at order p, the lfasm_asm_data arrays: dof and sign
+ * (ne * nd), fo (ne * 4, p >= 2; may be NULL at p = 1), J, Jinv (ne * 9
+ * row-major), detJ (ne), v0 (ne * 3), the DOF count *height and the sorted
+ * essential DOFs (every DOF of a face that one element alone references,
+ * with its edges) into ess (*n_ess of them; LFASM_ERR_ARG when more than
+ * ess_cap).  Element-local vertex order: ascending id, the last two
+ * swapped where that makes detJ > 0; edges and faces numbered by first
+ * occurrence (element-major, local edge / face order); a face's global
+ * vertex order is that of its first occurrence.  nv < 2^21. */
+int lfasm_extract(int gpu_id, int ne, int nv, int p, const int *tv, const double *xv, int *dof,
+                  double *sign, int *fo, double *J, double *Jinv, double *detJ, double *v0,
+                  int *ess, long long ess_cap, int *height, int *n_ess);
+
 /* Per-stage CUDA-event timing of lfasm_assemble (the analogue of the
  * reference's asm_gpu_*_s sub-timers, lithofem_solve.cpp:773-793):
  * lfasm_set_profile(h, 1) then, after an lfasm_assemble, ms3 receives the

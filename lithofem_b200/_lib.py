@@ -89,6 +89,10 @@ def lib() -> ct.CDLL:
         "lfasm_plane_orders": (ct.c_int, [H, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p,
                                           ct.POINTER(OrderPlaneC), ct.POINTER(OrderArgsC),
                                           ct.c_void_p, ct.c_void_p]),
+        "lfasm_extract": (ct.c_int, [ct.c_int, ct.c_int, ct.c_int, ct.c_int, c_int_p, c_double_p,
+                                     c_int_p, c_double_p, c_int_p, c_double_p, c_double_p,
+                                     c_double_p, c_double_p, c_int_p, ct.c_longlong,
+                                     ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]),
         "lfasm_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
         "lfasm_batch_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
         "lfasm_batch_assemble": (ct.c_int, [ct.c_void_p, ct.c_int]),

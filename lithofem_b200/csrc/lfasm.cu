@@ -31,6 +31,7 @@
 
 #include "../../include/lfasm.h"
 #include "lfasm_kernels.cuh"
+#include "lfextract.cuh"
 
 using namespace lfasm_dev;
 
@@ -1797,6 +1798,20 @@ namespace {
 
 // locate the nx x ny sample points of the plane z: element and reference
 // coordinates per point (device arrays owned by the caller afterwards)
+// Device buffers of one call, freed when it returns (on every path).
+struct DevBufs {
+  std::vector<void *> v;
+  ~DevBufs() {
+    for (void *q : v) dfree_bytes(q);
+  }
+  template <typename T>
+  cudaError_t get(T *&d, size_t n) {
+    cudaError_t e = dmalloc(d, n);
+    if (e == cudaSuccess) v.push_back((void *)d);
+    return e;
+  }
+};
+
 // Sample points of nz planes (heights zs, host) located in the mesh: per
 // plane the elements whose z-range holds it (flags [iz][e], one scan, one
 // compaction), then a warp per point over its plane's candidates; *elem
@@ -1984,6 +1999,165 @@ int lfasm_plane_orders(lfasm_handle *h, int nz, int nx, int ny, const void *d_e,
   LF_CUDA(cudaStreamSynchronize(h->stream));
   dfree(dp); dfree(dd); dfree(zs);
   return sync_if(h);
+}
+
+int lfasm_extract(int gpu_id, int ne, int nv, int p, const int *tv, const double *xv, int *dof,
+                  double *sign, int *fo, double *J, double *Jinv, double *detJ, double *v0,
+                  int *ess, long long ess_cap, int *height, int *n_ess) {
+  if (ne <= 0 || nv <= 0) return fail(LFASM_ERR_ARG, "empty mesh (%d elements, %d vertices)", ne, nv);
+  if (p < 1 || p > 3) return fail(LFASM_ERR_UNSUPPORTED, "order p = %d outside 1..3", p);
+  if (nv >= (1 << 21)) return fail(LFASM_ERR_ARG, "%d vertices: face keys hold 21 bits", nv);
+  if ((long long)ne * 6 >= INT_MAX / 2) return fail(LFASM_ERR_ARG, "%d elements: too many", ne);
+  if (!tv || !xv || !dof || !sign || (p >= 2 && !fo) || !J || !Jinv || !detJ || !v0 || !height ||
+      !n_ess || (ess_cap > 0 && !ess))
+    return fail(LFASM_ERR_ARG, "NULL argument");
+  for (long long i = 0; i < 4LL * ne; ++i)
+    if (tv[i] < 0 || tv[i] >= nv)
+      return fail(LFASM_ERR_ARG, "element %lld vertex %lld: id %d outside 0..%d", i / 4, i % 4,
+                  tv[i], nv - 1);
+  g_err.clear();
+  LF_CUDA(cudaSetDevice(gpu_id));
+  const int nd = p * (p + 2) * (p + 3) / 2;
+  DevBufs B;  // every device buffer of the call, freed on every return
+  cudaStream_t st = 0;
+  int *d_tvin, *d_tv, *d_err;
+  double *d_xv, *d_J, *d_Ji, *d_det, *d_v0;
+  LF_CUDA(B.get(d_tvin, (size_t)ne * 4));
+  LF_CUDA(B.get(d_tv, (size_t)ne * 4));
+  LF_CUDA(B.get(d_err, 2));
+  LF_CUDA(B.get(d_xv, (size_t)ne * 12));
+  LF_CUDA(B.get(d_J, (size_t)ne * 9));
+  LF_CUDA(B.get(d_Ji, (size_t)ne * 9));
+  LF_CUDA(B.get(d_det, (size_t)ne));
+  LF_CUDA(B.get(d_v0, (size_t)ne * 3));
+  LF_CUDA(cudaMemcpyAsync(d_tvin, tv, sizeof(int) * 4 * ne, cudaMemcpyHostToDevice, st));
+  LF_CUDA(cudaMemcpyAsync(d_xv, xv, sizeof(double) * 12 * ne, cudaMemcpyHostToDevice, st));
+  LF_CUDA(cudaMemsetAsync(d_err, 0, 2 * sizeof(int), st));
+  lfasm_ex::k_ex_local<<<(ne + 127) / 128, 128, 0, st>>>(ne, d_tvin, d_xv, d_tv, d_J, d_Ji, d_det,
+                                                          d_v0, d_err, d_err + 1);
+  LF_LAUNCHED();
+  int herr[2] = {0, 0};
+  LF_CUDA(cudaMemcpyAsync(herr, d_err, sizeof(herr), cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaStreamSynchronize(st));
+  if (herr[0] == lfasm_ex::EX_ERR_REPEATED)
+    return fail(LFASM_ERR_ARG, "element %d repeats a vertex", herr[1]);
+  if (herr[0]) return fail(LFASM_ERR_ARG, "element %d is degenerate (detJ <= 0)", herr[1]);
+
+  // ids by first occurrence of the key in row order (edges, then faces)
+  auto number = [&](long long n, unsigned long long *key, int *row, int *id, int **first_of,
+                    int **count_of, int *nuniq) -> int {
+    unsigned long long *ks;
+    int *rs, *head, *run, *rfirst, *rlen, *ridx, *sfirst, *srun, *rank;
+    LF_CUDA(B.get(ks, (size_t)n));
+    LF_CUDA(B.get(rs, (size_t)n));
+    LF_CUDA(B.get(head, (size_t)n));
+    LF_CUDA(B.get(run, (size_t)n));
+    size_t tb = 0, tb2 = 0;
+    LF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, ks, row, rs, (int)n, 0, 64, st));
+    LF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, head, run, (int)n, st));
+    unsigned char *tmp;
+    LF_CUDA(B.get(tmp, std::max(tb, tb2)));
+    tb = std::max(tb, tb2);
+    LF_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, ks, row, rs, (int)n, 0, 64, st));
+    const unsigned g = (unsigned)((n + 255) / 256);
+    lfasm_ex::k_ex_heads<<<g, 256, 0, st>>>(n, ks, head);
+    LF_LAUNCHED();
+    LF_CUDA(cub::DeviceScan::InclusiveSum(tmp, tb, head, run, (int)n, st));
+    int nrun = 0;
+    LF_CUDA(cudaMemcpyAsync(&nrun, run + n - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LF_CUDA(cudaStreamSynchronize(st));
+    LF_CUDA(B.get(rfirst, (size_t)nrun));
+    LF_CUDA(B.get(rlen, (size_t)nrun));
+    LF_CUDA(B.get(ridx, (size_t)nrun));
+    LF_CUDA(B.get(sfirst, (size_t)nrun));
+    LF_CUDA(B.get(srun, (size_t)nrun));
+    LF_CUDA(B.get(rank, (size_t)nrun));
+    LF_CUDA(B.get(*first_of, (size_t)nrun));
+    LF_CUDA(B.get(*count_of, (size_t)nrun));
+    LF_CUDA(cudaMemsetAsync(rlen, 0, sizeof(int) * nrun, st));
+    lfasm_ex::k_ex_runs<<<g, 256, 0, st>>>(n, head, run, rs, rfirst, rlen, ridx);
+    LF_LAUNCHED();
+    size_t tb3 = 0;
+    LF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb3, rfirst, sfirst, ridx, srun, nrun, 0, 32,
+                                            st));
+    unsigned char *tmp3;
+    LF_CUDA(B.get(tmp3, tb3));
+    LF_CUDA(cub::DeviceRadixSort::SortPairs(tmp3, tb3, rfirst, sfirst, ridx, srun, nrun, 0, 32,
+                                            st));
+    lfasm_ex::k_ex_rank<<<(nrun + 255) / 256, 256, 0, st>>>(nrun, srun, rank);
+    LF_LAUNCHED();
+    lfasm_ex::k_ex_ids<<<g, 256, 0, st>>>(n, run, rs, rank, rfirst, rlen, id, *first_of,
+                                          *count_of);
+    LF_LAUNCHED();
+    *nuniq = nrun;
+    return LFASM_OK;
+  };
+  const long long n6 = 6LL * ne, n4 = 4LL * ne;
+  unsigned long long *ekey, *fkey;
+  int *erow, *eid, *frow, *fid, *efirst, *ecount, *ffirst, *fcount, *d_fo, *d_dof, *flag, *pos;
+  signed char *esgn;
+  double *d_sign;
+  LF_CUDA(B.get(ekey, (size_t)n6));
+  LF_CUDA(B.get(erow, (size_t)n6));
+  LF_CUDA(B.get(eid, (size_t)n6));
+  LF_CUDA(B.get(esgn, (size_t)n6));
+  lfasm_ex::k_ex_edge_keys<<<(unsigned)((n6 + 255) / 256), 256, 0, st>>>(ne, d_tv, ekey, erow, esgn);
+  LF_LAUNCHED();
+  int nE = 0, nF = 0, rc;
+  if ((rc = number(n6, ekey, erow, eid, &efirst, &ecount, &nE))) return rc;
+  LF_CUDA(B.get(fkey, (size_t)n4));
+  LF_CUDA(B.get(frow, (size_t)n4));
+  LF_CUDA(B.get(fid, (size_t)n4));
+  LF_CUDA(B.get(d_fo, (size_t)n4));
+  lfasm_ex::k_ex_face_keys<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(ne, d_tv, fkey, frow);
+  LF_LAUNCHED();
+  if ((rc = number(n4, fkey, frow, fid, &ffirst, &fcount, &nF))) return rc;
+  lfasm_ex::k_ex_face_orient<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(ne, d_tv, fid, ffirst,
+                                                                          d_fo, d_err, d_err + 1);
+  LF_LAUNCHED();
+  const long long ndof_f = (long long)p * (p - 1), nint = nd - 6 * p - 4 * ndof_f;
+  const long long hgt = (long long)nE * p + nF * ndof_f + (long long)ne * nint;
+  if (hgt >= INT_MAX) return fail(LFASM_ERR_ARG, "%lld DOFs exceed 32-bit indices", hgt);
+  LF_CUDA(B.get(d_dof, (size_t)ne * nd));
+  LF_CUDA(B.get(d_sign, (size_t)ne * nd));
+  lfasm_ex::k_ex_dofs<<<(ne + 127) / 128, 128, 0, st>>>(ne, p, nd, nE * p, (int)(nF * ndof_f), eid,
+                                                         esgn, fid, d_fo, d_dof, d_sign);
+  LF_LAUNCHED();
+  LF_CUDA(B.get(flag, (size_t)hgt + 1));
+  LF_CUDA(B.get(pos, (size_t)hgt + 1));
+  LF_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (hgt + 1), st));
+  lfasm_ex::k_ex_ess<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(ne, p, nd, fid, fcount, d_dof,
+                                                                     flag);
+  LF_LAUNCHED();
+  size_t tb = 0;
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, (int)(hgt + 1), st));
+  unsigned char *tmp;
+  LF_CUDA(B.get(tmp, tb));
+  LF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, pos, (int)(hgt + 1), st));
+  int ness = 0;
+  LF_CUDA(cudaMemcpyAsync(&ness, pos + hgt, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(herr, d_err, sizeof(herr), cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaStreamSynchronize(st));
+  if (herr[0]) return fail(LFASM_ERR_ARG, "element %d: inconsistent face vertices", herr[1]);
+  *height = (int)hgt;
+  *n_ess = ness;
+  if (ness > ess_cap)
+    return fail(LFASM_ERR_ARG, "%d essential DOFs exceed the buffer of %lld", ness, ess_cap);
+  int *d_ess;
+  LF_CUDA(B.get(d_ess, (size_t)std::max(ness, 1)));
+  lfasm_ex::k_ex_compact<<<(unsigned)((hgt + 255) / 256), 256, 0, st>>>((int)hgt, flag, pos, d_ess);
+  LF_LAUNCHED();
+  LF_CUDA(cudaMemcpyAsync(dof, d_dof, sizeof(int) * ne * nd, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(sign, d_sign, sizeof(double) * ne * nd, cudaMemcpyDeviceToHost, st));
+  if (p >= 2)
+    LF_CUDA(cudaMemcpyAsync(fo, d_fo, sizeof(int) * 4 * ne, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(J, d_J, sizeof(double) * 9 * ne, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(Jinv, d_Ji, sizeof(double) * 9 * ne, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(detJ, d_det, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaMemcpyAsync(v0, d_v0, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, st));
+  if (ness) LF_CUDA(cudaMemcpyAsync(ess, d_ess, sizeof(int) * ness, cudaMemcpyDeviceToHost, st));
+  LF_CUDA(cudaStreamSynchronize(st));
+  return LFASM_OK;
 }
 
 int lfasm_set_profile(lfasm_handle *h, int on) {

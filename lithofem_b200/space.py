@@ -249,6 +249,49 @@ def build_asm_data(mesh: TetMesh, p: int, prob: Problem | None = None,
     return ad
 
 
+def build_asm_data_device(mesh: TetMesh, p: int, prob: Problem | None = None, gpu_id: int = 0,
+                          build_csr: bool = False) -> AsmData:
+    """build_asm_data (ascending local vertex order) with the extraction on
+    the device (lfasm_extract): local order, Jacobians, edge and face
+    numbering by first occurrence, face orientations, the DOF map and the
+    essential DOFs.  The integer arrays equal build_asm_data's; J and v0
+    too; Jinv and detJ come from the adjugate and agree to rounding."""
+    import ctypes as ct
+
+    from . import _lib
+    from ._abi import c_double_p, c_int_p
+    ne = mesh.ne
+    nd = nd_dofs(p)
+    tv = np.ascontiguousarray(mesh.tv, dtype=np.int32)
+    xv = np.ascontiguousarray(mesh.xv, dtype=np.float64)
+    dof = np.empty(ne * nd, dtype=np.int32)
+    sign = np.empty(ne * nd)
+    fo = np.empty(ne * 4 if p >= 2 else 0, dtype=np.int32)
+    J = np.empty(ne * 9)
+    Jinv = np.empty(ne * 9)
+    det = np.empty(ne)
+    v0 = np.empty(ne * 3)
+    cap = ne * nd
+    ess = np.empty(cap, dtype=np.int32)
+    height, n_ess = ct.c_int(), ct.c_int()
+    ip, dp = (lambda a: a.ctypes.data_as(c_int_p)), (lambda a: a.ctypes.data_as(c_double_p))
+    rc = _lib.lib().lfasm_extract(int(gpu_id), ne, int(mesh.nv), int(p), ip(tv), dp(xv), ip(dof),
+                                  dp(sign), ip(fo) if p >= 2 else None, dp(J), dp(Jinv), dp(det),
+                                  dp(v0), ip(ess), cap, ct.byref(height), ct.byref(n_ess))
+    _lib.check(rc)
+    ad = AsmData(
+        ne=ne, nd=nd, p=p, height=int(height.value),
+        has_kpar=bool(prob.has_kpar) if prob is not None else False,
+        dof=dof, sign=sign, fo=fo, attr=np.ascontiguousarray(mesh.attr.astype(np.int32)),
+        J=J, Jinv=Jinv, detJ=det, v0=v0,
+        rule_cc=_rule(p, max(0, 2 * p - 2)), rule_mass=_rule(p, 2 * p),
+        ess=ess[:n_ess.value].copy(),
+    )
+    if build_csr:
+        ad.I, ad.Jcol = csr_symbolic(ad)
+    return ad
+
+
 def csr_symbolic(ad: AsmData) -> tuple[np.ndarray, np.ndarray]:
     """Per-row sorted unique columns of the element DOF graph.
 
