@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--solve-only", action="store_true",
                     help="run only the solve+grad leg")
     ap.add_argument("--solve-reps", type=int, default=2)
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-meshes leg (the 16 polygon-hole meshes of --config 5 "
+                         "in one graph launch) of the default line")
     ap.add_argument("--pml-variant", type=int, default=-1,
                     help="force the PML kernel (0 k_pml_mma, 1 k_pml_ws at p = 3, 2 k_pml_sym); "
                          "default: autotune")
@@ -515,6 +518,11 @@ def run_ours(a, rank, world, local, dist, torch):
         assert g.SetAsync(False)
         solve = run_solve(a, case, dev, torch, g)
 
+    # the batched uneven meshes (the --config 5 workload) on the same GPU
+    batch = None
+    if not a.no_batch and world == 1:
+        batch = run_batch_leg(a, dev, torch, stream)
+
     if rank != 0:
         g.Release()
         if dist is not None:
@@ -590,7 +598,8 @@ def run_ours(a, rank, world, local, dist, torch):
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
             "config": cfg, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "roofline": roof, "cpu_baseline": cpu, "solve": solve, "kernels": kern,
+            "roofline": roof, "cpu_baseline": cpu, "solve": solve, "batch": batch,
+            "kernels": kern,
             "fp64_peak_tflops": fp64,
             "host_build_s": dict(case.host_s, what="host mesh generation and space / per-mesh "
                                  "data extraction (build_asm_data) of this mesh, once per "
@@ -763,6 +772,48 @@ def run_e2e(a, case, dev, torch, stream) -> dict | None:
             "timer": "host wall clock with device synchronize on both sides",
             "breakdown_ms": {"init": br[0], "build_global": br[1], "assemble": br[2],
                              "d2h": br[3], "release": br[4]}}
+
+
+def run_batch_leg(a, dev, torch, stream) -> dict:
+    """The 16 polygon-hole meshes of --config 5 assembled by one graph launch
+    (lfasm_batch_assemble) on this GPU, device-timed like the main line:
+    value = total nnz / time per launch; the meshes' host build apart."""
+    from lithofem_b200 import _lib, configs
+    from lithofem_b200.asm import AsmBatch, AsmGpuGlobal
+    t0 = time.perf_counter()
+    cases = configs.batch_config(scale=a.scale)
+    t_build = time.perf_counter() - t0
+    hs = []
+    for c in cases:
+        h = AsmGpuGlobal(c.prob)
+        assert h.Init(c.ad, dev) and h.BuildGlobal(c.ad.ess)
+        c.nnz = h.nnz()
+        assert h.Assemble(True)          # tunes the handle
+        hs.append(h)
+    b = AsmBatch(hs)
+    assert b.SetStream(stream.cuda_stream)
+    for _ in range(max(3, a.warmup)):
+        assert b.Assemble(True)
+    torch.cuda.synchronize()
+    launches0 = _lib.lib().lfasm_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        assert b.Assemble(True)
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = _lib.lib().lfasm_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1) / a.steps
+    b.Release()
+    for h in hs:
+        h.Release()
+    total = sum(c.nnz for c in cases)
+    cfg = batch_workload_config(cases, a)
+    cfg.pop("meshes")
+    return {"metric": METRIC, "value": total / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "steps": a.steps, "config": cfg, "gpu_launches_per_step": launches / a.steps,
+            "host_build_s": t_build,
+            "timer": "CUDA events on the launching stream around the graph launches"}
 
 
 def batch_workload_config(cases, a) -> dict:
