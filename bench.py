@@ -187,7 +187,8 @@ class ClockSampler:
 PML_KERNELS = ["k_pml_mma", "k_pml_ws", "k_pml_sym"]
 BULK_KERNELS = ["k_bulk (SIMT)", "k_bulk_mma<4 tiles/warp> (DMMA)", "k_bulk_mma<2 tiles/warp> (DMMA)",
                 "k_bulk_mma_nb<4 tiles/warp> (DMMA, no block barriers)",
-                "k_bulk_mma_nb<2 tiles/warp> (DMMA, no block barriers)"]
+                "k_bulk_mma_nb<2 tiles/warp> (DMMA, no block barriers)",
+                "k_bulk_tma<4 tiles/warp> (DMMA, records staged by cp.async.bulk)"]
 
 
 def pml_flops(n_pml: int, nd: int, nq_cc: int, nq_mass: int, cross: bool, variant: int) -> float:

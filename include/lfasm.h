@@ -234,7 +234,9 @@ int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_
 
 /* Autotuner: times the bulk-element kernel variants on this mesh -- 0: the
  * SIMT k_bulk, 1 and 2: the FP64 tensor-core k_bulk_mma with 4 or 2 tiles
- * per warp, 3 and 4: the same without block barriers (k_bulk_mma_nb) -- and
+ * per warp, 3 and 4: the same without block barriers (k_bulk_mma_nb), 5:
+ * k_bulk_mma with 4 tiles per warp and the element records staged into
+ * shared memory by the bulk-copy engine (k_bulk_tma) -- and
  * keeps the fastest.  The first lfasm_assemble of a handle
  * whose variant was not set takes the decision from a per-process cache
  * keyed by device, order p, k-parallel terms and the power-of-two class of
@@ -242,7 +244,7 @@ int lfasm_eps_gradient(lfasm_handle *h, const lfasm_incident_part *parts, int n_
  * lfasm_autotune always times and refreshes the cache.  lfasm_get_tuning
  * reports the choice and one timing per variant (ms, LFASM_BULK_VARIANTS
  * floats). */
-#define LFASM_BULK_VARIANTS 5
+#define LFASM_BULK_VARIANTS 6
 int lfasm_autotune(lfasm_handle *h);
 int lfasm_set_bulk_variant(lfasm_handle *h, int variant);
 int lfasm_get_tuning(lfasm_handle *h, int *bulk_variant, float *ms);

@@ -14,7 +14,7 @@ c_int_p = ct.POINTER(ct.c_int)
 c_double_p = ct.POINTER(ct.c_double)
 
 CURLCURL, MASS, CROSS0, CROSS1, KLK = 1, 2, 4, 8, 16
-BULK_VARIANTS = 5   # LFASM_BULK_VARIANTS: bulk-element kernel variants of the autotuner
+BULK_VARIANTS = 6   # LFASM_BULK_VARIANTS: bulk-element kernel variants of the autotuner
 ERR_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_UNSUPPORTED", 4: "ERR_STATE",
              5: "ERR_CSR"}
 

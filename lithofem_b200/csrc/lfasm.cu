@@ -311,12 +311,14 @@ int sync_if(lfasm_handle *h) {
   if (!h->async_mode) {
     LF_CUDA(cudaStreamSynchronize(h->stream));
     if (int rb = bounds_status()) return rb;
-    if (h->pml_variant == 1 && h->err) {
+    if ((h->pml_variant == 1 || h->bulk_variant == 5) && h->err) {
       int e = 0;
       LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
       if (e) {
         LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
-        return fail(LFASM_ERR_CUDA, "PML pipeline: a bounded wait ran out (results undefined)");
+        return fail(LFASM_ERR_CUDA,
+                    "PML pipeline or staged bulk records: a bounded wait ran out (results "
+                    "undefined)");
       }
     }
   }
@@ -954,8 +956,9 @@ static int launch_bulk(lfasm_handle *h, int mask, int te, int mode, int eliminat
     }
     if (!body) return LFASM_OK;
     const int ntiles = bulk_tiles(h->ndp);
-    const int TT = (h->bulk_variant == 1 || h->bulk_variant == 3) ? 4 : 2;  // tiles per warp
-    const bool nobar = h->bulk_variant >= 3;
+    const int TT = (h->bulk_variant == 2 || h->bulk_variant == 4) ? 2 : 4;  // tiles per warp
+    const bool nobar = h->bulk_variant == 3 || h->bulk_variant == 4;
+    const bool tma = h->bulk_variant == 5;
     const int ytiles = (ntiles + BULK_WARPS * TT - 1) / (BULK_WARPS * TT);
     // k_bulk_mma writes 16-byte-aligned double4 pairs: needs rs even (the
     // fused layout); the dense ComputeLocal layout uses the SIMT kernel
@@ -964,10 +967,19 @@ static int launch_bulk(lfasm_handle *h, int mask, int te, int mode, int eliminat
     const int bchunk = (int)std::max<long long>(1, ((long long)nbat * ytiles + want - 1) / want);
     dim3 grid((nbat + bchunk - 1) / bchunk, ytiles);
 #define LF_BULKM(C, M, T, F)                                                      \
-  (nobar ? k_bulk_mma_nb<C, M, T, F> : k_bulk_mma<C, M, T, F>)                    \
-      <<<grid, BULK_WARPS * 32, 0, st>>>(                                         \
-      nb, blist, recm, F ? h->S_mmaf : h->S_mma, ntiles, h->nd, h->ndp, \
-      h->p, bchunk, te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae)
+  do {                                                                            \
+    if (tma)                                                                      \
+      k_bulk_tma<C, M, T, F><<<grid, BULK_WARPS * 32, 0, st>>>(                   \
+          nb, blist, recm, F ? h->S_mmaf : h->S_mma, ntiles, h->nd, h->ndp, h->p, \
+          bchunk, te, eliminate, rs, h->fopack, h->signmask, h->essmask, h->Ae,   \
+          h->err);                                                                \
+    else                                                                          \
+      (nobar ? k_bulk_mma_nb<C, M, T, F> : k_bulk_mma<C, M, T, F>)                \
+          <<<grid, BULK_WARPS * 32, 0, st>>>(                                     \
+          nb, blist, recm, F ? h->S_mmaf : h->S_mma, ntiles, h->nd, h->ndp,       \
+          h->p, bchunk, te, eliminate, rs, h->fopack, h->signmask, h->essmask,    \
+          h->Ae);                                                                 \
+  } while (0)
 #define LF_BULKM_T(T, F)                                                          \
   do {                                                                            \
     if (cross) { if (mode) LF_BULKM(true, 1, T, F); else LF_BULKM(true, 0, T, F); }   \
@@ -1366,9 +1378,15 @@ int lfasm_autotune(lfasm_handle *h) {
     }
   }
   h->n_pml = keep_n_pml;
+  int ebulk = 0;
+  if (!rc) {
+    // the staged-record variant (5) is never chosen if one of its waits ran out
+    LF_CUDA(cudaMemcpy(&ebulk, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ebulk) LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+  }
   int best = 0;
   for (int v = 1; v < LFASM_BULK_VARIANTS; ++v)
-    if (h->tune_ms[v] < h->tune_ms[best]) best = v;
+    if (h->tune_ms[v] < h->tune_ms[best] && !(v == 5 && ebulk)) best = v;
   h->bulk_variant = best;
   if (!rc && h->n_pml > 0 && !h->pml_forced) {
     // PML kernels (the warp-specialised one at p = 3 only), the PML path alone
@@ -1752,12 +1770,12 @@ int lfasm_batch_assemble(lfasm_batch *b, int eliminate) {
   if (int rb = bounds_status()) return rb;
   for (size_t i = 0; i < b->hs.size(); ++i) {
     lfasm_handle *h = b->hs[i];
-    if (h->pml_variant != 1) continue;
+    if (h->pml_variant != 1 && h->bulk_variant != 5) continue;
     int e = 0;
     LF_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
       LF_CUDA(cudaMemset(h->err, 0, sizeof(int)));
-      return fail(LFASM_ERR_CUDA, "handle %zu: PML pipeline: a bounded wait ran out", i);
+      return fail(LFASM_ERR_CUDA, "handle %zu: a bounded wait ran out", i);
     }
   }
   return LFASM_OK;

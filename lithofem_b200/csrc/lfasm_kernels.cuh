@@ -1411,6 +1411,145 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// k_bulk_mma with the element records staged by the bulk-copy engine: thread
+// 0 issues one cp.async.bulk (global -> shared, completion counted on an
+// mbarrier in bytes) per batch of 8 elements, one batch ahead into the other
+// of two shared buffers, so the records reach shared memory without passing
+// through registers.  Every wait on a copy is bounded (a wait that runs out
+// sets *err, skips the rest of its waits and the block still finishes);
+// before returning, thread 0 waits (bounded) for any copy still in flight.
+// Same tiles, operands and epilogue as k_bulk_mma.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// bytes (a multiple of 16) from src (16-byte aligned) to the 16-byte aligned
+// shared dst, completion on bar
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <bool CROSS, int MODE, int TT, bool FUSED>
+__global__ void __launch_bounds__(BULK_WARPS * 32)
+k_bulk_tma(int nb, const int *__restrict__ list, const double *__restrict__ rec,
+           const double *__restrict__ S, int ntiles, int nd, int ndp, int p, int bchunk, int te,
+           int eliminate, int rs, const unsigned *__restrict__ fopack,
+           const unsigned long long *__restrict__ signmask,
+           const unsigned long long *__restrict__ essmask, dcplx *__restrict__ Ae,
+           int *__restrict__ err) {
+  constexpr int PB = TT / 2;
+  constexpr int KS = FUSED ? 7 : BK / 4;
+  constexpr int RECW = FUSED ? BK : BREC;
+  __shared__ alignas(128) double sA[2][8 * RECW];
+  __shared__ unsigned long long bar[2];
+  __shared__ double sT[24];
+  __shared__ int se[8];
+  __shared__ unsigned sfo[8];
+  __shared__ unsigned long long ssm[8], sem[8];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int ncb = (ndp + 7) / 8;
+  const int npb = (ndp / 2) * ncb;
+  if (tid < 24) sT[tid] = c_tinv[tid];
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
+  double bf[PB][2][KS];
+  int rowv[PB], colv[PB], frv[PB], fcv[PB], okv[PB];
+  const int pb0 = (blockIdx.y * BULK_WARPS + w) * PB;
+#pragma unroll
+  for (int j = 0; j < PB; ++j) {
+    const int pb = pb0 + j;
+    const bool ok = pb < npb;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      const int tile = 2 * pb + a;
+#pragma unroll
+      for (int ks = 0; ks < KS; ++ks)
+        bf[j][a][ks] = ok ? S[(size_t)(ks * 4 + t4) * ntiles * 8 + tile * 8 + g] : 0.0;
+    }
+    const int I = ok ? pb / ncb : 0, cb = ok ? pb - I * ncb : 0;
+    rowv[j] = 2 * I;
+    colv[j] = 8 * cb + 2 * t4;
+    okv[j] = ok && rowv[j] < nd && colv[j] < nd;
+    frv[j] = (te && p >= 2) ? face_of(2 * I, p) : -1;
+    fcv[j] = (te && p >= 2) ? face_of(colv[j], p) : -1;
+  }
+  const int nbat = (nb + 7) / 8;
+  const int b0 = blockIdx.x * bchunk, b1 = min(nbat, b0 + bchunk);
+  // batch bt goes to buffer (bt - b0) & 1, the k-th use of a buffer
+  // completing its barrier's phase k & 1
+  auto issue = [&](int bt) {
+    const int ebase = bt * 8, nel = min(8, nb - ebase), buf = (bt - b0) & 1;
+    const unsigned bytes = (unsigned)(nel * RECW * sizeof(double));
+    // the buffer's previous contents were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[buf], bytes);
+    bulk_g2s(sA[buf], rec + (size_t)ebase * RECW, bytes, &bar[buf]);
+  };
+  int pfe = -1;
+  unsigned pfo = 0u;
+  unsigned long long psm = 0ull, pem = 0ull;
+  auto meta = [&](int bt) {
+    const int ebase = bt * 8;
+    const int nel = bt < b1 ? min(8, nb - ebase) : 0;
+    pfe = tid < nel ? list[ebase + tid] : -1;
+    if (pfe >= 0) {
+      pfo = fopack[pfe];
+      psm = MODE == 1 ? signmask[pfe] : 0ull;
+      pem = (MODE == 1 && eliminate) ? essmask[pfe] : 0ull;
+    }
+  };
+  __syncthreads();  // barriers initialised
+  if (tid == 0 && b0 < b1) issue(b0);
+  meta(b0);
+  bool live = true;
+  for (int bt = b0; bt < b1; ++bt) {
+    const int buf = (bt - b0) & 1;
+    const unsigned par = (unsigned)(((bt - b0) >> 1) & 1);
+    __syncthreads();  // the previous batch is done: its buffer may be refilled
+    if (tid < 8) {
+      se[tid] = pfe;
+      sfo[tid] = pfe >= 0 ? pfo : 0u;
+      ssm[tid] = pfe >= 0 ? psm : 0ull;
+      sem[tid] = pfe >= 0 ? pem : 0ull;
+    }
+    if (tid == 0 && bt + 1 < b1) issue(bt + 1);
+    __syncthreads();
+    meta(bt + 1);
+    if (live) live = mbar_wait(&bar[buf], par, err);
+    const double *A = sA[buf];
+    double ar[3], ai[KS];
+#pragma unroll
+    for (int ks = 0; ks < 3; ++ks) ar[ks] = A[g * RECW + ks * 4 + t4];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks)
+      ai[ks] = FUSED ? (ks >= 3 ? A[g * RECW + ks * 4 + t4] : 0.0) : A[g * RECW + BK + ks * 4 + t4];
+    const int e = se[g];
+    const unsigned fp = sfo[g];
+    const unsigned long long sm = ssm[g], em = sem[g];
+    dcplx *base = e >= 0 ? Ae + (size_t)e * nd * rs : Ae;
+#pragma unroll
+    for (int j = 0; j < PB; ++j)
+      bulk_rowpair<CROSS, MODE, KS, FUSED>(bf[j], ar, ai, okv[j] && e >= 0, fp, sm, em, rowv[j],
+                                           colv[j], frv[j], fcv[j], sT, nd, rs, base);
+  }
+  // a copy whose wait ran out may still be in flight: drain the last use of
+  // each buffer before the block's shared memory is released
+  if (!live && tid == 0)
+    for (int last = b1 - 1; last >= b0 && last >= b1 - 2; --last)
+      mbar_wait(&bar[(last - b0) & 1], (unsigned)(((last - b0) >> 1) & 1), err);
+}
+
 struct PmlWsShape {
   static constexpr int NDP8 = 48, LD = 52, MT = 6, QC = 8, RMAX = 6 * QC;
   static constexpr size_t BUF = (size_t)3 * RMAX * LD;  // doubles per ring buffer

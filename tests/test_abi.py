@@ -157,7 +157,7 @@ def test_tuning_entry_points_reject_a_null_handle():
         assert rc == 1 and b"NULL handle" in L.lfasm_last_error()
     header = (Path(__file__).resolve().parents[1] / "include" / "lfasm.h").read_text()
     n = int(re.search(r"#define LFASM_BULK_VARIANTS (\d+)", header).group(1))
-    assert n == _abi.BULK_VARIANTS == 5
+    assert n == _abi.BULK_VARIANTS == 6
 
 
 def test_no_cpu_fallback(tmp_path):

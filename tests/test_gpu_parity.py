@@ -225,7 +225,8 @@ def test_against_reference_cuda_kernels(kcase):
 
 
 @pytest.mark.parametrize("kcase", [("grating", 3, 6.0), ("hole", 2, 0.0), ("hole", 1, 6.0), ("slab", 3, 6.0)], ids=ids)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4], ids=["simt", "dmma4", "dmma2", "nb4", "nb2"])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5],
+                         ids=["simt", "dmma4", "dmma2", "nb4", "nb2", "tma4"])
 def test_bulk_variants(kcase, variant):
     """Every bulk-element kernel (the autotuner's candidates) matches the oracle."""
     c = case(*kcase) if kcase[0] != "slab" else configs.small_case("slab", 3, 6.0, seed=13, h=3.2)
@@ -308,8 +309,8 @@ def test_autotuner_picks_a_variant():
     g = AsmGpuGlobal(c.prob)
     assert g.Init(c.ad, 0) and g.BuildGlobal(c.ad.ess) and g.Assemble(True)
     v, ms = g.Tuning()
-    assert len(ms) == 5 and v in range(5) and min(ms) > 0 and ms[v] == min(ms)
-    assert not g.SetBulkVariant(5) and g.last_error[0] == 1
+    assert len(ms) == 6 and v in range(6) and min(ms) > 0 and ms[v] == min(ms)
+    assert not g.SetBulkVariant(6) and g.last_error[0] == 1
 
 
 def test_high_valence_row():
