@@ -94,7 +94,14 @@ int lfsolve_solve(lfsolve *s, int nrhs, const void *d_b, void *d_x, int transpos
  * (LFSOLVE_ERR_NOCONV, with *rel set, if the tolerance is not reached).
  * rel_out (nrhs doubles, may be NULL) receives the final relative residuals
  * and *iters_out (may be NULL) the corrections applied.  transpose != 0
- * solves A^T x = b (residual with A^T). */
+ * solves A^T x = b (residual with A^T).  When a correction reduces the
+ * worst relative residual by less than half (refinement stalls, e.g. when
+ * the factors are far from A), the solve switches to GMRES-based
+ * refinement: per column, restarted GMRES(30) on A x = b in FP64 from the
+ * current x, right-preconditioned by the factors, up to 10 max_iter Arnoldi
+ * steps; *iters_out then counts the corrections plus the Arnoldi steps.
+ * The environment variable LFSOLVE_GMRES=1 uses GMRES from the start,
+ * LFSOLVE_GMRES=0 never. */
 int lfsolve_solve_refined(lfsolve *s, const int *d_I, const int *d_J, const void *d_vals,
                           int nrhs, const void *d_b, void *d_x, int transpose, double tol,
                           int max_iter, double *rel_out, int *iters_out);

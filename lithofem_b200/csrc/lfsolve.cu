@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -591,6 +592,28 @@ __global__ void k_swap_cols_batched(const EaItem *__restrict__ items,
       col[q] = t;
     }
   }
+}
+
+// y = A x (or A^T x through the transposed positions) in FP64, a warp per
+// row; one column
+__global__ void k_spmv(int n, const int *__restrict__ I, const int *__restrict__ J,
+                       const double2 *__restrict__ vals, const int *__restrict__ tpos,
+                       const double2 *__restrict__ x, double2 *__restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= n) return;
+  double ar = 0.0, ai = 0.0;
+  for (int p = I[row] + lane; p < I[row + 1]; p += 32) {
+    const double2 a = vals[tpos ? tpos[p] : p];
+    const double2 xv = x[J[p]];
+    ar = fma(a.x, xv.x, ar); ar = fma(-a.y, xv.y, ar);
+    ai = fma(a.x, xv.y, ai); ai = fma(a.y, xv.x, ai);
+  }
+  for (int o = 16; o; o >>= 1) {
+    ar += __shfl_xor_sync(0xffffffffu, ar, o);
+    ai += __shfl_xor_sync(0xffffffffu, ai, o);
+  }
+  if (lane == 0) y[row] = make_double2(ar, ai);
 }
 
 // Error-compensated TF32 operands of F22 -= L21 U12 (complex64, kk pivot
@@ -1729,6 +1752,133 @@ int solve_dispatch(lfsolve *s, int nrhs, const double2 *b, double2 *x, int trans
                                 : solve_any<cuDoubleComplex>(s, nrhs, b, x, trans, d_scale, accumulate);
 }
 
+// GMRES-IR for one column: restarted GMRES(m) on A x = b in FP64 (complex128
+// vectors, modified Gram-Schmidt Arnoldi, complex Givens rotations), right
+// preconditioned by the factors (M^-1 v: one triangular solve of the
+// factorization's precision), from the current x.  The Krylov basis, the
+// Hessenberg solve and the update x += M^-1 (V y) follow the standard
+// algorithm (Saad and Schultz 1986; with a low-precision preconditioner,
+// Carson and Higham's GMRES-based iterative refinement, 2017-2018).  *iters
+// counts the Arnoldi steps; *rel is the final true relative residual.
+int gmres_column(lfsolve *s, const int *d_I, const int *d_J, const double2 *vals, const int *tp,
+                 const double2 *b, double2 *x, int trans, double tol, int max_steps, int m,
+                 double *rel, int *iters) {
+  using cd = std::complex<double>;
+  const int n = s->P.n;
+  cudaStream_t st = s->stream;
+  int rc = ensure_lanes(s);
+  if (rc) return rc;
+  cublasHandle_t hb = s->blas_main;
+  LS_BLAS(cublasSetPointerMode(hb, CUBLAS_POINTER_MODE_HOST));
+  double2 *V = nullptr, *z = nullptr, *w = nullptr;
+  LS_CUDA(cudaMalloc((void **)&V, sizeof(double2) * (size_t)n * (m + 1)));
+  LS_CUDA(cudaMalloc((void **)&z, sizeof(double2) * (size_t)n));
+  LS_CUDA(cudaMalloc((void **)&w, sizeof(double2) * (size_t)n));
+  struct Free {
+    void *a, *b, *c;
+    ~Free() { cudaFree(a); cudaFree(b); cudaFree(c); }
+  } guard{V, z, w};
+  auto spmv = [&](const double2 *in, double2 *out) -> int {
+    k_spmv<<<(n + 7) / 8, 256, 0, st>>>(n, d_I, d_J, vals, tp, in, out);
+    LS_CUDA(cudaGetLastError());
+    return LFSOLVE_OK;
+  };
+  auto zc = [](cuDoubleComplex v) { return cd(v.x, v.y); };
+  auto cz = [](cd v) { return make_cuDoubleComplex(v.real(), v.imag()); };
+  double bn = 0.0;
+  LS_BLAS(cublasDznrm2(hb, n, reinterpret_cast<const cuDoubleComplex *>(b), 1, &bn));
+  if (bn == 0.0) bn = 1.0;
+  std::vector<cd> H((size_t)(m + 1) * m), g(m + 1), sn(m), y(m);
+  std::vector<double> cs(m);
+  int steps = 0;
+  *rel = 1.0;
+  while (true) {
+    // r = b - A x into V[0]
+    if ((rc = spmv(x, w))) return rc;
+    LS_CUDA(cudaMemcpyAsync(V, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, st));
+    const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
+    auto *V0 = reinterpret_cast<cuDoubleComplex *>(V);
+    LS_BLAS(cublasZaxpy(hb, n, &mone, reinterpret_cast<const cuDoubleComplex *>(w), 1, V0, 1));
+    double beta = 0.0;
+    LS_BLAS(cublasDznrm2(hb, n, V0, 1, &beta));
+    *rel = beta / bn;
+    if (*rel <= tol || steps >= max_steps || beta == 0.0) break;
+    const double ib = 1.0 / beta;
+    LS_BLAS(cublasZdscal(hb, n, &ib, V0, 1));
+    std::fill(g.begin(), g.end(), cd(0.0));
+    g[0] = beta;
+    int k = 0;
+    for (; k < m && steps < max_steps; ++k) {
+      auto *Vk = reinterpret_cast<cuDoubleComplex *>(V + (size_t)k * n);
+      // w = A M^-1 v_k
+      if ((rc = solve_dispatch(s, 1, reinterpret_cast<const double2 *>(Vk), z, trans, nullptr, 0)))
+        return rc;
+      if ((rc = spmv(z, w))) return rc;
+      auto *W = reinterpret_cast<cuDoubleComplex *>(w);
+      for (int i = 0; i <= k; ++i) {
+        auto *Vi = reinterpret_cast<cuDoubleComplex *>(V + (size_t)i * n);
+        cuDoubleComplex hij;
+        LS_BLAS(cublasZdotc(hb, n, Vi, 1, W, 1, &hij));
+        H[(size_t)i * m + k] = zc(hij);
+        const cuDoubleComplex neg = make_cuDoubleComplex(-hij.x, -hij.y);
+        LS_BLAS(cublasZaxpy(hb, n, &neg, Vi, 1, W, 1));
+      }
+      double hn = 0.0;
+      LS_BLAS(cublasDznrm2(hb, n, W, 1, &hn));
+      H[(size_t)(k + 1) * m + k] = hn;
+      if (hn > 0.0) {
+        const double ih = 1.0 / hn;
+        LS_CUDA(cudaMemcpyAsync(V + (size_t)(k + 1) * n, w, sizeof(double2) * n,
+                                cudaMemcpyDeviceToDevice, st));
+        LS_BLAS(cublasZdscal(hb, n, &ih,
+                             reinterpret_cast<cuDoubleComplex *>(V + (size_t)(k + 1) * n), 1));
+      }
+      // earlier rotations on column k, then the one that zeroes H[k+1][k]
+      for (int i = 0; i < k; ++i) {
+        const cd a = H[(size_t)i * m + k], c = H[(size_t)(i + 1) * m + k];
+        H[(size_t)i * m + k] = cs[i] * a + sn[i] * c;
+        H[(size_t)(i + 1) * m + k] = -std::conj(sn[i]) * a + cs[i] * c;
+      }
+      const cd a = H[(size_t)k * m + k];
+      const double bb = hn, r = std::hypot(std::abs(a), bb);
+      if (std::abs(a) == 0.0) {
+        cs[k] = 0.0;
+        sn[k] = 1.0;
+        H[(size_t)k * m + k] = bb;
+      } else {
+        const cd ph = a / std::abs(a);
+        cs[k] = std::abs(a) / r;
+        sn[k] = ph * bb / r;
+        H[(size_t)k * m + k] = ph * r;
+      }
+      H[(size_t)(k + 1) * m + k] = 0.0;
+      g[k + 1] = -std::conj(sn[k]) * g[k];
+      g[k] = cs[k] * g[k];
+      ++steps;
+      if (std::abs(g[k + 1]) / bn <= 0.5 * tol || hn == 0.0) {
+        ++k;
+        break;
+      }
+    }
+    // y = H^-1 g (upper triangular k x k), u = V y, x += M^-1 u
+    for (int i = k - 1; i >= 0; --i) {
+      cd t = g[i];
+      for (int j = i + 1; j < k; ++j) t -= H[(size_t)i * m + j] * y[j];
+      y[i] = t / H[(size_t)i * m + i];
+    }
+    LS_CUDA(cudaMemsetAsync(w, 0, sizeof(double2) * n, st));
+    for (int i = 0; i < k; ++i) {
+      const cuDoubleComplex yi = cz(y[i]);
+      LS_BLAS(cublasZaxpy(hb, n, &yi, reinterpret_cast<const cuDoubleComplex *>(V + (size_t)i * n),
+                          1, reinterpret_cast<cuDoubleComplex *>(w), 1));
+    }
+    if ((rc = solve_dispatch(s, 1, w, x, trans, nullptr, 1))) return rc;
+  }
+  *iters = steps;
+  LS_CUDA(cudaStreamSynchronize(st));
+  return LFSOLVE_OK;
+}
+
 void free_factors(lfsolve *s) {
   if (s->d_fac) cudaFree(s->d_fac);
   s->d_fac = nullptr;
@@ -1921,22 +2071,48 @@ int lfsolve_solve_refined(lfsolve *s, const int *d_I, const int *d_J, const void
   int rc = solve_dispatch(s, nrhs, b, x, transpose != 0, nullptr, 0);
   if (rc) return rc;
   double worst = 0.0;
-  int it = 0;
+  int it = 0, steps = 0;
   if ((rc = residual(&worst))) return rc;
-  while (worst > tol && it < max_iter) {
+  // classical refinement while it contracts; when a correction reduces the
+  // worst residual by less than half (or LFSOLVE_GMRES=1 asks for it from
+  // the start), GMRES-IR takes over, column by column, with up to
+  // 10 max_iter Arnoldi steps (LFSOLVE_GMRES=0: never)
+  const char *ge = std::getenv("LFSOLVE_GMRES");
+  bool gmres = ge && ge[0] == '1';
+  const bool no_gmres = ge && ge[0] == '0';  // classical refinement only
+  // (comparisons written so that a NaN residual counts as not converged)
+  while (!gmres && !(worst <= tol) && it < max_iter) {
     LS_CUDA(cudaMemcpyAsync(s->d_scale, sc.data(), sizeof(double) * 2 * nrhs, cudaMemcpyHostToDevice, st));
     if ((rc = solve_dispatch(s, nrhs, s->d_r, x, transpose != 0, s->d_scale, 1))) return rc;
     ++it;
+    const double prev = worst;
+    if ((rc = residual(&worst))) return rc;
+    if (!(worst <= tol) && !(worst <= 0.5 * prev) && !no_gmres) gmres = true;
+  }
+  if (gmres && !(worst <= tol)) {
+    // a diverged refinement leaves x worse than zero: start from x = 0
+    if (!(worst < 1.0)) LS_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * (size_t)n * nrhs, st));
+    for (int c = 0; c < nrhs; ++c) {
+      double rel = 0.0;
+      int k = 0;
+      if ((rc = gmres_column(s, d_I, d_J, static_cast<const double2 *>(d_vals), tp,
+                             b + (size_t)c * n, x + (size_t)c * n, transpose != 0, tol,
+                             10 * std::max(1, max_iter), 30, &rel, &k)))
+        return rc;
+      steps += k;
+    }
     if ((rc = residual(&worst))) return rc;
   }
+  it += steps;
   LS_CUDA(cudaEventRecord(s->t1, st));
   LS_CUDA(cudaStreamSynchronize(st));
   LS_CUDA(cudaEventElapsedTime(&s->st.solve_ms, s->t0, s->t1));
   s->st.refine_iters = it;
   s->st.refine_rel = worst;
   if (iters_out) *iters_out = it;
-  if (worst > tol)
-    return fail(LFSOLVE_ERR_NOCONV, "refinement stopped at relative residual %.3e after %d corrections",
+  if (!(worst <= tol))
+    return fail(LFSOLVE_ERR_NOCONV,
+                "refinement stopped at relative residual %.3e after %d corrections / GMRES steps",
                 worst, it);
   return LFSOLVE_OK;
 }

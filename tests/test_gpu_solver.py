@@ -247,3 +247,56 @@ def test_tf32x3_schur_updates_refine_to_1e10(kcase, monkeypatch):
     assert ok and max(rel) <= 1e-10, (s.last_error, rel, it)
     assert rel_err(x.cpu().numpy(), x128.cpu().numpy()) <= 1e-8
     s.Release()
+
+
+@pytest.mark.parametrize("transpose", [False, True], ids=["A", "AT"])
+def test_gmres_ir_forced_from_the_start(transpose, monkeypatch):
+    """GMRES-based refinement (restarted GMRES(30) in FP64, right
+    preconditioned by the complex64 factors) reaches 1e-10 and agrees with
+    the complex128 solution, for A and for A^T."""
+    import torch
+    c, g, b = system(("grating", 2, 6.0))
+    s = DirectSolver(0)
+    assert s.AnalyzeAssembly(g, c.ad) and s.FactorDevice(g._csr()[2], C128)
+    xref = torch.empty_like(b)
+    assert s.Backsolve(2, b.data_ptr(), xref.data_ptr(), transpose)
+    assert s.FactorDevice(g._csr()[2], C64)
+    monkeypatch.setenv("LFSOLVE_GMRES", "1")
+    x = torch.empty_like(b)
+    ok, rel, it = s.SolveRefined(g, 2, b.data_ptr(), x.data_ptr(), transpose, 1e-10)
+    assert ok and max(rel) <= 1e-10, (s.last_error, rel, it)
+    assert 1 <= it <= 60
+    assert rel_err(x.cpu().numpy(), xref.cpu().numpy()) <= 1e-8
+    s.Release()
+
+
+def test_gmres_ir_takes_over_when_refinement_stalls(monkeypatch):
+    """Factors of a perturbed matrix (every value times 1 + d u, u uniform in
+    [-1, 1]): at the first d where classical refinement alone no longer
+    converges, the automatic switch to GMRES-IR still reaches 1e-10 on the
+    true matrix."""
+    import torch
+    c, g, b = system(("grating", 2, 6.0))
+    V = g.DownloadValues()
+    rng = np.random.default_rng(21)
+    u = rng.uniform(-1.0, 1.0, V.shape)
+    s = DirectSolver(0)
+    assert s.AnalyzeAssembly(g, c.ad)
+    x = torch.empty_like(b)
+    seen = []
+    for d in (1e-4, 1e-3, 3e-3, 1e-2, 3e-2):
+        Vp = torch.from_numpy(V * (1.0 + d * u)).cuda()
+        assert s.FactorDevice(Vp.data_ptr(), C64)
+        monkeypatch.setenv("LFSOLVE_GMRES", "0")
+        ok_ir, rel_ir, it_ir = s.SolveRefined(g, 2, b.data_ptr(), x.data_ptr(), False, 1e-10)
+        monkeypatch.delenv("LFSOLVE_GMRES")
+        ok, rel, it = s.SolveRefined(g, 2, b.data_ptr(), x.data_ptr(), False, 1e-10)
+        seen.append((d, ok_ir, max(rel_ir), it_ir, ok, max(rel), it))
+        print(f"perturbation {d:.0e}: refinement alone ok={ok_ir} rel={max(rel_ir):.2e} "
+              f"({it_ir}); with GMRES-IR ok={ok} rel={max(rel):.2e} ({it})")
+        if not ok_ir:
+            assert ok and max(rel) <= 1e-10, seen
+            break
+    else:
+        pytest.fail(f"refinement converged at every perturbation: {seen}")
+    s.Release()
