@@ -84,10 +84,13 @@ inline long long align_up(long long x) { return (x + ALIGN - 1) / ALIGN * ALIGN;
 constexpr int FPAD = 16;
 inline int pad_up(int x) { return (x + FPAD - 1) / FPAD * FPAD; }
 
-// fronts with at most SMALL_M rows (and 2 k + r <= SMALL_BWD) are solved by
-// one block each, with the right-hand-side block in shared memory: m x nrhs
-// entries forward, (2 k + r) x nrhs backward, at most 196 kB in complex128
+// fronts with at most SMALL_M rows, SMALL_K pivots and 2 k + r <= SMALL_BWD
+// are solved by one block each, with the right-hand-side block in shared
+// memory: m x nrhs entries forward, (2 k + r) x nrhs backward, at most
+// 192 kB in complex128 (two right-hand sides a pass); the block takes one
+// barrier per pivot, so fronts with more pivots go to the library path
 constexpr int SMALL_M = 4096;
+constexpr int SMALL_K = 256;
 constexpr int SMALL_BWD = 6144;
 constexpr int SOLVE_THREADS = 256;
 constexpr int MAX_NRHS_PASS = 2;  // right-hand sides per solve pass
@@ -926,6 +929,54 @@ __global__ void k_laswp(int k, const int *__restrict__ ipiv, T *__restrict__ v, 
   }
 }
 
+// Pivot permutation of every front: the front's sequential row swaps
+// (ipiv, 1-based) applied to the identity, so that the swapped vector is
+// v[perm[i]] at row i and the inverse swaps put row i at perm[i]; a block
+// per front, the swaps in shared memory up to cap pivots (global beyond)
+constexpr int PERM_CAP = 12288;
+__global__ void k_ipiv_to_perm(const NodeDev *__restrict__ nodes, const int *__restrict__ ipiv,
+                               int *__restrict__ perm) {
+  __shared__ int sp[PERM_CAP];
+  const NodeDev N = nodes[blockIdx.x];
+  const int k = N.k;
+  int *dst = perm + N.p0;
+  const int *pv = ipiv + N.p0;
+  int *w = k <= PERM_CAP ? sp : dst;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) w[i] = i;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int q = 0; q < k; ++q) {
+      const int p = pv[q] - 1;
+      if (p != q && p >= 0 && p < k) {
+        const int t = w[q];
+        w[q] = w[p];
+        w[p] = t;
+      }
+    }
+  __syncthreads();
+  if (k <= PERM_CAP)
+    for (int i = threadIdx.x; i < k; i += blockDim.x) dst[i] = sp[i];
+}
+
+// big fronts: the pivot rows of a vector block permuted (INV = 0: row i
+// takes row perm[i]; INV = 1: row i goes to perm[i]); a block per column,
+// the k rows staged in shared memory
+template <typename T, int INV>
+__global__ void k_perm_pivots(int k, const int *__restrict__ perm, T *__restrict__ v, int ldv) {
+  extern __shared__ unsigned char perm_sm[];
+  T *sv = reinterpret_cast<T *>(perm_sm);
+  T *vc = v + (long long)blockIdx.x * ldv;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) sv[i] = vc[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    if (INV) vc[perm[i]] = sv[i];
+    else vc[i] = sv[perm[i]];
+  }
+}
+// pivots of a vector block that the shared-memory permutation can take
+template <typename T>
+constexpr int perm_smem_max() { return (int)(160 * 1024 / sizeof(T)); }
+
 // big fronts: x_R gathered into a dense block (r x nrhs, ld r), and the
 // pivots' solution scattered back to x
 template <typename T>
@@ -1149,6 +1200,7 @@ struct lfsolve {
   int prec = -1;
   void *d_fac = nullptr;
   int *d_ipiv = nullptr, *d_info = nullptr;
+  int *d_pperm = nullptr;  // per-front pivot permutations (from d_ipiv)
   // lanes
   cudaStream_t lane[LANES] = {};
   cublasHandle_t blas[LANES] = {};
@@ -1188,7 +1240,9 @@ int upload(T **dst, const std::vector<T> &v, cudaStream_t st) {
   return LFSOLVE_OK;
 }
 
-bool is_small(const Node &N) { return N.m <= SMALL_M && 2 * N.k + (N.m - N.k) <= SMALL_BWD; }
+bool is_small(const Node &N) {
+  return N.m <= SMALL_M && N.k <= SMALL_K && 2 * N.k + (N.m - N.k) <= SMALL_BWD;
+}
 
 int ensure_uploaded(lfsolve *s) {
   if (s->uploaded) return LFSOLVE_OK;
@@ -1278,6 +1332,15 @@ int ensure_lanes(lfsolve *s) {
   if (s->blas_main) return LFSOLVE_OK;
   LS_BLAS(cublasCreate(&s->blas_main));
   LS_BLAS(cublasSetStream(s->blas_main, s->stream));
+  // the vector permutations stage up to 160 kB of pivot rows
+  LS_CUDA(cudaFuncSetAttribute(k_perm_pivots<cuComplex, 0>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+  LS_CUDA(cudaFuncSetAttribute(k_perm_pivots<cuComplex, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+  LS_CUDA(cudaFuncSetAttribute(k_perm_pivots<cuDoubleComplex, 0>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+  LS_CUDA(cudaFuncSetAttribute(k_perm_pivots<cuDoubleComplex, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
   for (int l = 0; l < LANES; ++l) {
     LS_CUDA(cudaStreamCreateWithFlags(&s->lane[l], cudaStreamNonBlocking));
     LS_BLAS(cublasCreate(&s->blas[l]));
@@ -1588,7 +1651,11 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
         const T *Pf = fac + N.fac_off;
         const T *U12 = Pf + (long long)m * k;
         if (!trans) {
-          k_laswp<T, 0><<<1, 32, 0, s->lane[l]>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
+          if (k <= perm_smem_max<T>())
+            k_perm_pivots<T, 0><<<nr, 1024, (size_t)k * sizeof(T), s->lane[l]>>>(
+                k, s->d_pperm + N.p0, v, (int)VR);
+          else
+            k_laswp<T, 0><<<1, 32, 0, s->lane[l]>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
           LS_CUDA(cudaGetLastError());
           LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
                        CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
@@ -1664,7 +1731,11 @@ int solve_pass(lfsolve *s, int nr, const T *b, T *x, int trans) {
                          (int)VR));
           LS_BLAS(trsm(bh, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
                        CUBLAS_DIAG_UNIT, k, nr, &one, Pf, m, v, (int)VR));
-          k_laswp<T, 1><<<1, 32, 0, ls>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
+          if (k <= perm_smem_max<T>())
+            k_perm_pivots<T, 1><<<nr, 1024, (size_t)k * sizeof(T), ls>>>(
+                k, s->d_pperm + N.p0, v, (int)VR);
+          else
+            k_laswp<T, 1><<<1, 32, 0, ls>>>(k, s->d_ipiv + N.p0, v, (int)VR, nr);
           LS_CUDA(cudaGetLastError());
         }
         k_scatter_pivots<T><<<grid_for(k, 256), 256, 0, ls>>>(k, s->d_perm + N.p0, v, VR, x, n, nr);
@@ -1987,6 +2058,11 @@ int lfsolve_factor(lfsolve *s, const void *d_vals, int prec) {
   rc = prec == LFSOLVE_C64 ? factor_impl<cuComplex>(s, static_cast<const double2 *>(d_vals))
                            : factor_impl<cuDoubleComplex>(s, static_cast<const double2 *>(d_vals));
   if (rc) return rc;
+  // the fronts' pivot permutations for the solves' row interchanges
+  if (!s->d_pperm) LS_CUDA(cudaMalloc((void **)&s->d_pperm, sizeof(int) * std::max(1, s->P.nn)));
+  k_ipiv_to_perm<<<(unsigned)s->P.nodes.size(), 128, 0, s->stream>>>(s->d_nodes, s->d_ipiv,
+                                                                      s->d_pperm);
+  LS_CUDA(cudaGetLastError());
   LS_CUDA(cudaEventRecord(s->t1, s->stream));
   LS_CUDA(cudaStreamSynchronize(s->stream));
   LS_CUDA(cudaEventElapsedTime(&s->st.factor_ms, s->t0, s->t1));
@@ -2134,7 +2210,8 @@ void lfsolve_destroy(lfsolve *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_factors(s);
   void *bufs[] = {s->d_nodes, s->d_child, s->d_rel, s->d_perm, s->d_rorig, s->d_ess, s->d_tpos,
-                  s->d_ipiv, s->d_info, s->d_V, s->d_bw, s->d_xr, s->d_r, s->d_part, s->d_scale};
+                  s->d_ipiv, s->d_info, s->d_V, s->d_bw, s->d_xr, s->d_r, s->d_part, s->d_scale,
+                  s->d_pperm};
   for (void *p : bufs)
     if (p) cudaFree(p);
   for (auto *p : s->d_asm_src) if (p) cudaFree(p);
