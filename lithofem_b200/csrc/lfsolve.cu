@@ -639,15 +639,18 @@ __device__ __forceinline__ void tf32_split(cuComplex v, float2 &h, float2 &l) {
   h = make_float2(tf32_round(v.x), tf32_round(v.y));
   l = make_float2(v.x - h.x, v.y - h.y);
 }
+// nb fronts of the same shape: front f's block at L + f sL, its operand at
+// A + f sA (B + f sB)
 __global__ void k_split_a(int r, int kk, const cuComplex *__restrict__ L, int ld,
-                          float *__restrict__ A, int lda) {
-  const long long n = (long long)r * kk, lo_off = (long long)2 * kk * lda;
+                          float *__restrict__ A, int lda, int nb, long long sL, long long sA) {
+  const long long per = (long long)r * kk, n = per * nb, lo_off = (long long)2 * kk * lda;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % r), j = (int)(t / r);
+    const long long f = t / per, u = t - f * per;
+    const int i = (int)(u % r), j = (int)(u / r);
     float2 h, l;
-    tf32_split(L[i + (long long)j * ld], h, l);
-    float *c0 = A + (long long)(2 * j) * lda + 2 * i;  // column 2j; 2j + 1 one lda on
+    tf32_split(L[f * sL + i + (long long)j * ld], h, l);
+    float *c0 = A + f * sA + (long long)(2 * j) * lda + 2 * i;  // column 2j; 2j + 1 one lda on
     *reinterpret_cast<float2 *>(c0) = h;
     *reinterpret_cast<float2 *>(c0 + lda) = make_float2(-h.y, h.x);
     *reinterpret_cast<float2 *>(c0 + lo_off) = l;
@@ -655,14 +658,15 @@ __global__ void k_split_a(int r, int kk, const cuComplex *__restrict__ L, int ld
   }
 }
 __global__ void k_split_b(int kk, int r, const cuComplex *__restrict__ U, int ld,
-                          float *__restrict__ B) {
-  const long long n = (long long)kk * r;
+                          float *__restrict__ B, int nb, long long sU, long long sB) {
+  const long long per = (long long)kk * r, n = per * nb;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(t % kk), c = (int)(t / kk);
+    const long long f = t / per, u = t - f * per;
+    const int j = (int)(u % kk), c = (int)(u / kk);
     float2 h, l;
-    tf32_split(U[j + (long long)c * ld], h, l);
-    float *col = B + (long long)c * 4 * kk;
+    tf32_split(U[f * sU + j + (long long)c * ld], h, l);
+    float *col = B + f * sB + (long long)c * 4 * kk;
     *reinterpret_cast<float2 *>(col + 2 * j) = l;
     *reinterpret_cast<float2 *>(col + 2 * kk + 2 * j) = h;
   }
@@ -1410,9 +1414,9 @@ int schur_tf32x3(lfsolve *s, int l, cuComplex *F, int ld, int kk, int r) {
   float *A = static_cast<float *>(s->split[l]);
   float *B = A + na;
   const int g = grid_for((long long)r * kk, 256);
-  k_split_a<<<g, 256, 0, s->lane[l]>>>(r, kk, F + kk, ld, A, (int)lda);
+  k_split_a<<<g, 256, 0, s->lane[l]>>>(r, kk, F + kk, ld, A, (int)lda, 1, 0, 0);
   LS_CUDA(cudaGetLastError());
-  k_split_b<<<g, 256, 0, s->lane[l]>>>(kk, r, F + (long long)kk * ld, ld, B);
+  k_split_b<<<g, 256, 0, s->lane[l]>>>(kk, r, F + (long long)kk * ld, ld, B, 1, 0, 0);
   LS_CUDA(cudaGetLastError());
   const float mone = -1.f, one = 1.f;
   float *C = reinterpret_cast<float *>(F + kk + (long long)kk * ld);
@@ -1422,6 +1426,37 @@ int schur_tf32x3(lfsolve *s, int l, cuComplex *F, int ld, int kk, int r) {
   LS_BLAS(cublasGemmEx(s->blas[l], CUBLAS_OP_N, CUBLAS_OP_N, 2 * r, r, 2 * kk, &mone, A,
                        CUDA_R_32F, (int)lda, B + 2 * kk, CUDA_R_32F, 4 * kk, &one, C,
                        CUDA_R_32F, 2 * ld, CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+  return LFSOLVE_OK;
+}
+
+// The same for all cnt fronts of a batched depth (uniform kk x r blocks,
+// front stride S entries, leading dimension ld) on the main stream, the
+// split operands in the solver's pool for the duration of the call
+int schur_tf32x3_batched(lfsolve *s, cuComplex *arena, long long S, int ld, int kk, int r,
+                         int cnt) {
+  cudaStream_t st = s->stream;
+  const long long lda = ((2LL * r + 31) / 32) * 32;
+  const long long na = lda * 4 * kk, nbf = 4LL * kk * r;
+  float *A = nullptr;
+  LS_CUDA(cudaMallocFromPoolAsync((void **)&A, sizeof(float) * (size_t)(na + nbf) * cnt, s->pool,
+                                  st));
+  float *B = A + na * cnt;
+  const int g = grid_for((long long)r * kk * cnt, 256);
+  k_split_a<<<g, 256, 0, st>>>(r, kk, arena + kk, ld, A, (int)lda, cnt, S, na);
+  LS_CUDA(cudaGetLastError());
+  k_split_b<<<g, 256, 0, st>>>(kk, r, arena + (long long)kk * ld, ld, B, cnt, S, nbf);
+  LS_CUDA(cudaGetLastError());
+  const float mone = -1.f, one = 1.f;
+  float *C = reinterpret_cast<float *>(arena + kk + (long long)kk * ld);
+  LS_BLAS(cublasGemmStridedBatchedEx(s->blas_main, CUBLAS_OP_N, CUBLAS_OP_N, 2 * r, r, 4 * kk,
+                                     &mone, A, CUDA_R_32F, (int)lda, na, B, CUDA_R_32F, 4 * kk,
+                                     nbf, &one, C, CUDA_R_32F, 2 * ld, 2 * S, cnt,
+                                     CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+  LS_BLAS(cublasGemmStridedBatchedEx(s->blas_main, CUBLAS_OP_N, CUBLAS_OP_N, 2 * r, r, 2 * kk,
+                                     &mone, A, CUDA_R_32F, (int)lda, na, B + 2 * kk, CUDA_R_32F,
+                                     4 * kk, nbf, &one, C, CUDA_R_32F, 2 * ld, 2 * S, cnt,
+                                     CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+  LS_CUDA(cudaFreeAsync(A, st));
   return LFSOLVE_OK;
 }
 
@@ -1486,9 +1521,15 @@ int factor_impl(lfsolve *s, const double2 *vals) {
                              CUBLAS_DIAG_UNIT, kp, rp, &one, p11, ld, p12, ld, cnt));
         LS_BLAS(trsm_batched(s->blas_main, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
                              CUBLAS_DIAG_NON_UNIT, rp, kp, &one, p11, ld, p21, ld, cnt));
-        LS_BLAS(gemm_sb(s->blas_main, rp, rp, kp, &mone, arena[d] + kp, ld, S,
-                        arena[d] + (long long)kp * ld, ld, S, &one,
-                        arena[d] + kp + (long long)kp * ld, ld, S, cnt));
+        if (use_tf32x3<T>(s) && (double)rp * rp * kp * cnt >= tf32x3_min()) {
+          int rc3 = schur_tf32x3_batched(s, reinterpret_cast<cuComplex *>(arena[d]), S, ld, kp, rp,
+                                         cnt);
+          if (rc3) return rc3;
+        } else {
+          LS_BLAS(gemm_sb(s->blas_main, rp, rp, kp, &mone, arena[d] + kp, ld, S,
+                          arena[d] + (long long)kp * ld, ld, S, &one,
+                          arena[d] + kp + (long long)kp * ld, ld, S, cnt));
+        }
       }
       if (s->n_co[d] > 0) {
         k_copy_out<T><<<s->n_co[d], 256, 0, st>>>(s->d_co[d], s->d_nodes, arena[d], fac);

@@ -226,16 +226,17 @@ def test_batched_depths_equal_per_front_factorization(kcase, monkeypatch):
     assert max(e_b, e_p) <= 1e-2 and max(e_b, e_p) <= 10 * min(e_b, e_p) + 1e-6, (e_b, e_p)
 
 
+@pytest.mark.parametrize("batch_min", ["100000", "4"], ids=["per-front", "batched"])
 @pytest.mark.parametrize("kcase", [("grating", 3, 6.0), ("hole", 3, 0.0)], ids=["grating-p3", "hole-p3"])
-def test_tf32x3_schur_updates_refine_to_1e10(kcase, monkeypatch):
+def test_tf32x3_schur_updates_refine_to_1e10(kcase, batch_min, monkeypatch):
     """Large complex64 fronts update their Schur complement with three TF32
     tensor-core GEMMs on split operands (about 2^-22 relative); forced on
-    every front of the per-front path here, the refined solve still reaches
-    1e-10 and agrees with the complex128 solution."""
+    every front, on the per-front path and on the batched depths (strided
+    batched GEMMs), the refined solve still reaches 1e-10 and agrees with
+    the complex128 solution."""
     import torch
     c, g, b = system(kcase)
-    n = c.ad.height
-    monkeypatch.setenv("LFSOLVE_BATCH_MIN", "100000")
+    monkeypatch.setenv("LFSOLVE_BATCH_MIN", batch_min)
     s = DirectSolver(0)
     assert s.AnalyzeAssembly(g, c.ad) and s.FactorDevice(g._csr()[2], C128)
     x128 = torch.empty_like(b)
