@@ -938,13 +938,8 @@ __global__ void k_laswp(int k, const int *__restrict__ ipiv, T *__restrict__ v, 
 // v[perm[i]] at row i and the inverse swaps put row i at perm[i]; a block
 // per front, the swaps in shared memory up to cap pivots (global beyond)
 constexpr int PERM_CAP = 12288;
-__global__ void k_ipiv_to_perm(const NodeDev *__restrict__ nodes, const int *__restrict__ ipiv,
-                               int *__restrict__ perm) {
-  __shared__ int sp[PERM_CAP];
-  const NodeDev N = nodes[blockIdx.x];
-  const int k = N.k;
-  int *dst = perm + N.p0;
-  const int *pv = ipiv + N.p0;
+__device__ void perm_from_ipiv(int k, const int *__restrict__ pv, int *__restrict__ dst,
+                               int *__restrict__ sp) {
   int *w = k <= PERM_CAP ? sp : dst;
   for (int i = threadIdx.x; i < k; i += blockDim.x) w[i] = i;
   __syncthreads();
@@ -960,6 +955,29 @@ __global__ void k_ipiv_to_perm(const NodeDev *__restrict__ nodes, const int *__r
   __syncthreads();
   if (k <= PERM_CAP)
     for (int i = threadIdx.x; i < k; i += blockDim.x) dst[i] = sp[i];
+}
+__global__ void k_ipiv_to_perm(const NodeDev *__restrict__ nodes, const int *__restrict__ ipiv,
+                               int *__restrict__ perm) {
+  __shared__ int sp[PERM_CAP];
+  const NodeDev N = nodes[blockIdx.x];
+  perm_from_ipiv(N.k, ipiv + N.p0, perm + N.p0, sp);
+}
+// one front's permutation (k pivots at pv) into perm
+__global__ void k_ipiv_to_perm_one(int k, const int *__restrict__ pv, int *__restrict__ perm) {
+  __shared__ int sp[PERM_CAP];
+  perm_from_ipiv(k, pv, perm, sp);
+}
+// the factorization's row interchanges on the ncol update columns of a
+// front (A: the first k rows of column c at A + c ld): a block per column,
+// the k rows staged in shared memory, row i taking row perm[i]
+template <typename T>
+__global__ void k_perm_cols(int k, const int *__restrict__ perm, T *__restrict__ A, int ld) {
+  extern __shared__ unsigned char pc_sm[];
+  T *sv = reinterpret_cast<T *>(pc_sm);
+  T *col = A + (long long)blockIdx.x * ld;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) sv[i] = col[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < k; i += blockDim.x) col[i] = sv[perm[i]];
 }
 
 // big fronts: the pivot rows of a vector block permuted (INV = 0: row i
@@ -1345,6 +1363,10 @@ int ensure_lanes(lfsolve *s) {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
   LS_CUDA(cudaFuncSetAttribute(k_perm_pivots<cuDoubleComplex, 1>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+  LS_CUDA(cudaFuncSetAttribute(k_perm_cols<cuComplex>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+  LS_CUDA(cudaFuncSetAttribute(k_perm_cols<cuDoubleComplex>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
   for (int l = 0; l < LANES; ++l) {
     LS_CUDA(cudaStreamCreateWithFlags(&s->lane[l], cudaStreamNonBlocking));
     LS_BLAS(cublasCreate(&s->blas[l]));
@@ -1586,8 +1608,14 @@ int factor_impl(lfsolve *s, const double2 *vals) {
       LS_CUDA(cudaMemcpyAsync(s->d_ipiv + N.p0, s->lpiv[l], sizeof(int) * k,
                               cudaMemcpyDeviceToDevice, s->lane[l]));
       if (r > 0) {
-        k_swap_cols<T><<<(r + 127) / 128, 128, 0, s->lane[l]>>>(k, r, s->d_ipiv + N.p0,
-                                                                F + (long long)kk * ld, ld);
+        if (k <= perm_smem_max<T>()) {
+          k_ipiv_to_perm_one<<<1, 256, 0, s->lane[l]>>>(k, s->d_ipiv + N.p0, s->lpiv[l]);
+          k_perm_cols<T><<<r, 256, (size_t)k * sizeof(T), s->lane[l]>>>(
+              k, s->lpiv[l], F + (long long)kk * ld, ld);
+        } else {
+          k_swap_cols<T><<<(r + 127) / 128, 128, 0, s->lane[l]>>>(k, r, s->d_ipiv + N.p0,
+                                                                  F + (long long)kk * ld, ld);
+        }
         LS_CUDA(cudaGetLastError());
         LS_BLAS(trsm(s->blas[l], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
                      CUBLAS_DIAG_UNIT, kk, r, &one, F, ld, F + (long long)kk * ld, ld));
