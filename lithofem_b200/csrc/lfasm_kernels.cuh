@@ -1758,6 +1758,12 @@ k_pml_ws(int npml, const int *__restrict__ list, int nd, int rs, int p, Rule rcc
 // the row's own CSR values for rows longer than the shared accumulator),
 // the unit diagonal of an essential row set.  Inlined twice so that the
 // shared-memory path keeps shared-memory instructions.
+// row-list entries whose element-row loads a gather warp issues together
+// (2 measured best on the benchmark mesh: 0.96 ms against 1.04 for 1 and
+// 1.22 for 4, whose registers cost occupancy)
+#ifndef GATHER_UNROLL
+#define GATHER_UNROLL 2
+#endif
 template <bool RAW>
 __device__ __forceinline__ void gather_row_q(dcplx *acc, int r, int rb, int nr, int lane,
                                              int p0, int p1, bool row_ess,
@@ -1791,6 +1797,46 @@ __device__ __forceinline__ void gather_row_q(dcplx *acc, int r, int rb, int nr, 
       }
       for (int t = 0; t < epi; ++t) {
         if (sub == t && j >= 0) { acc[j].re += v.re; acc[j].im += v.im; }
+        __syncwarp();
+      }
+    }
+  } else if (!RAW && nd <= 64 && GATHER_UNROLL > 1) {
+    // GATHER_UNROLL row-list entries a step: every lane loads its columns of
+    // all of them first (independent loads in flight together), then the
+    // additions go entry by entry (two entries may share a slot)
+    constexpr int U = GATHER_UNROLL;
+    for (int q0 = p0; q0 < p1; q0 += U) {
+      dcplx v[U][2];
+      int j[U][2];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int pp = q0 + u;
+        j[u][0] = j[u][1] = -1;
+        if (pp < p1) {
+          const int id = ea[pp];
+          if (LF_CHECK(id >= 0 && id < n_erows, BOUNDS_ELEM_ROW)) {
+            const dcplx *src = Ae + (size_t)id * rs;
+            const uint16_t *o = off + (size_t)pp * nd;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int b = lane + 32 * h;
+              if (b < nd) {
+                v[u][h] = src[b];
+                const int jj = o[b];
+                j[u][h] = LF_CHECK(jj < nr, BOUNDS_SLOT) ? jj : -1;
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (j[u][h] >= 0) {
+            acc[j[u][h]].re += v[u][h].re;
+            acc[j[u][h]].im += v[u][h].im;
+          }
         __syncwarp();
       }
     }
