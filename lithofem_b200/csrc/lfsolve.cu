@@ -30,6 +30,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -37,8 +38,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lfsolve.h"
@@ -119,6 +122,21 @@ struct Node {
                               // padded pivot count of a batched depth)
 };
 
+// host array of n values left uninitialised (filled by the caller), the
+// assembly map's hundreds of MB not zeroed first
+template <typename T>
+struct HostBuf {
+  std::unique_ptr<T[]> p;
+  size_t n = 0;
+  void resize(size_t m) { p.reset(m ? new T[m] : nullptr); n = m; }
+  T *data() { return p.get(); }
+  const T *data() const { return p.get(); }
+  T &operator[](size_t i) { return p[i]; }
+  const T &operator[](size_t i) const { return p[i]; }
+  size_t size() const { return n; }
+  bool empty() const { return n == 0; }
+};
+
 struct Plan {
   int n = 0, n_ess = 0, nn = 0;       // rows, essential rows, numbered rows
   long long nnz = 0;
@@ -140,9 +158,9 @@ struct Plan {
   std::vector<long long> stride;
   std::vector<int> ess;
   // assembly map per depth: CSR position -> arena offset
-  std::vector<std::vector<int>> asm_src;
-  std::vector<std::vector<long long>> asm_dst;
-  std::vector<int> tpos;              // CSR position of the transposed entry
+  std::vector<HostBuf<int>> asm_src;        // every entry is written: no zero fill
+  std::vector<HostBuf<long long>> asm_dst;
+  HostBuf<int> tpos;                  // CSR position of the transposed entry
   double flops = 0.0;
   int max_front = 0, max_k = 0, max_depth = 0;
   long long peak_front_entries = 0;
@@ -224,6 +242,25 @@ void bisect(int n, int ne, int nd, const int *edof, const double *cen,
   }
 }
 
+// f(item, worker) for every item of [0, n) on the host threads, items handed
+// out one at a time (the fronts' work varies by orders of magnitude)
+template <typename F>
+void parallel_items(int n, F f) {
+  int T = (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
+  T = std::max(1, std::min(T, n));
+  std::atomic<int> next{0};
+  auto run = [&](int w) {
+    for (int i = next++; i < n; i = next++) f(i, w);
+  };
+  if (T == 1) { run(0); return; }
+  std::vector<std::thread> th;
+  for (int w = 0; w < T; ++w) th.emplace_back(run, w);
+  for (auto &t : th) t.join();
+}
+inline int host_workers(int n) {
+  return std::max(1, std::min((int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())), n));
+}
+
 int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
                const int *edof, const double *cen, const int *ess, int n_ess, int leaf,
                Plan &P) {
@@ -240,8 +277,20 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
   P.n_ess = (int)P.ess.size();
   for (long long t = 0; t < (long long)ne * nd; ++t)
     if (edof[t] < 0 || edof[t] >= n) return fail(LFSOLVE_ERR_ARG, "element DOF %d out of range", edof[t]);
+  // LFSOLVE_PROFILE set: host seconds of the analysis phases printed
+  const bool prof = std::getenv("LFSOLVE_PROFILE") != nullptr;
+  auto tick = std::chrono::steady_clock::now();
+  auto phase = [&](const char *what) {
+    if (!prof) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::printf("lfsolve analysis: %-28s %8.3f s\n", what,
+                std::chrono::duration<double>(now - tick).count());
+    std::fflush(stdout);
+    tick = now;
+  };
   std::vector<int> owner, elems;
   bisect(n, ne, nd, edof, cen, is_ess, leaf, P, owner, elems);
+  phase("nested dissection");
   for (int i = 0; i < n; ++i)
     if (!is_ess[i] && owner[i] < 0)
       return fail(LFSOLVE_ERR_ARG, "row %d is touched by no element", i);
@@ -305,6 +354,7 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
     const double k = N.k, r = (double)N.R.size();
     P.flops += 8.0 * (k * k * k / 3.0 + k * k * r + k * r * r);
   }
+  phase("numbering, update rows");
   // layouts
   P.by_depth.assign(P.max_depth + 1, {});
   for (int s : P.post) P.by_depth[P.nodes[s].depth].push_back(s);
@@ -386,47 +436,98 @@ int build_plan(int n, const int *I, const int *J, long long nnz, int ne, int nd,
     for (int t = 0; t < N.k; ++t) loc[N.p0 + t] = -1;
     for (int v : N.R) loc[v] = -1;
   }
-  // transposed positions (the structure must be symmetric)
-  P.tpos.assign(nnz, -1);
+  phase("layouts, child row maps");
+  // transposed positions: entry (i, j) -> the position of (j, i), by binary
+  // search in row j (columns sorted); the structure must be symmetric
+  P.tpos.resize(nnz);  // every entry written below (or the call fails)
   {
-    std::vector<long long> cnt(n, 0);
-    for (int i = 0; i < n; ++i)
-      for (long long p = I[i]; p < I[i + 1]; ++p) {
-        const int j = J[p];
-        const long long q = I[j] + cnt[j]++;
-        if (q >= I[j + 1] || J[q] != i)
-          return fail(LFSOLVE_ERR_ARG, "the CSR structure is not symmetric (row %d, column %d)", i, j);
-        P.tpos[p] = (int)q;
-      }
+    std::atomic<long long> bad{-1};
+    constexpr int ROWS = 4096;  // rows an item
+    parallel_items((n + ROWS - 1) / ROWS, [&](int it, int) {
+      for (int i = it * ROWS; i < std::min(n, (it + 1) * ROWS); ++i)
+        for (long long p = I[i]; p < I[i + 1]; ++p) {
+          const int j = J[p];
+          const int *b = J + I[j], *e = J + I[j + 1];
+          const int *f = std::lower_bound(b, e, i);
+          if (f == e || *f != i) {
+            long long expect = -1;
+            bad.compare_exchange_strong(expect, (long long)i << 32 | (unsigned)j);
+            return;
+          }
+          P.tpos[p] = (int)(f - J);
+        }
+    });
+    if (bad >= 0)
+      return fail(LFSOLVE_ERR_ARG, "the CSR structure is not symmetric (row %d, column %d)",
+                  (int)(bad >> 32), (int)(bad & 0xffffffff));
   }
-  // assembly map
-  P.asm_src.assign(P.max_depth + 1, {});
-  P.asm_dst.assign(P.max_depth + 1, {});
-  for (int s = 0; s < ns; ++s) {
-    const Node &N = P.nodes[s];
-    for (int t = 0; t < N.k; ++t) loc[N.p0 + t] = t;
-    for (size_t t = 0; t < N.R.size(); ++t) loc[N.R[t]] = N.roff + (int)t;
-    auto &src = P.asm_src[N.depth];
-    auto &dst = P.asm_dst[N.depth];
-    for (int t = 0; t < N.k; ++t) {
-      const int i = P.perm[N.p0 + t];
-      const long long li = t;
-      for (long long p = I[i]; p < I[i + 1]; ++p) {
-        const int vj = P.iperm[J[p]];
-        if (vj < N.p0) continue;  // essential, or eliminated further down
-        const long long lj = loc[vj];
-        if (lj < 0) return fail(LFSOLVE_ERR_ARG, "internal: coupling outside the front");
-        src.push_back((int)p);
-        dst.push_back(N.arena_off + li + lj * N.ld);
-        if (vj >= N.p0 + N.k) {
-          src.push_back(P.tpos[p]);
-          dst.push_back(N.arena_off + lj + li * N.ld);
+  phase("transposed positions");
+  // assembly map: every entry (i, j) with i eliminated at front s and j not
+  // eliminated before it goes to its front position (and the transposed
+  // entry, when j is an update row); per depth, fronts in index order, each
+  // front's entries in row order.  A counting pass sizes every front's
+  // slice, then the fronts fill their slices on the host threads.
+  P.asm_src.clear();
+  P.asm_src.resize(P.max_depth + 1);
+  P.asm_dst.clear();
+  P.asm_dst.resize(P.max_depth + 1);
+  {
+    const int W = host_workers(ns);
+    std::vector<std::vector<int>> wloc(W, std::vector<int>(P.nn, -1));
+    std::vector<long long> cnt(ns, 0), off(ns, 0);
+    parallel_items(ns, [&](int s, int) {
+      const Node &N = P.nodes[s];
+      long long c = 0;
+      for (int t = 0; t < N.k; ++t) {
+        const int i = P.perm[N.p0 + t];
+        for (long long p = I[i]; p < I[i + 1]; ++p) {
+          const int vj = P.iperm[J[p]];
+          if (vj < N.p0) continue;  // essential, or eliminated further down
+          c += vj >= N.p0 + N.k ? 2 : 1;
         }
       }
+      cnt[s] = c;
+    });
+    std::vector<long long> total(P.max_depth + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+      off[s] = total[P.nodes[s].depth];
+      total[P.nodes[s].depth] += cnt[s];
     }
-    for (int t = 0; t < N.k; ++t) loc[N.p0 + t] = -1;
-    for (int v : N.R) loc[v] = -1;
+    for (int d = 0; d <= P.max_depth; ++d) {
+      P.asm_src[d].resize(total[d]);
+      P.asm_dst[d].resize(total[d]);
+    }
+    std::atomic<int> outside{0};
+    parallel_items(ns, [&](int s, int w) {
+      const Node &N = P.nodes[s];
+      std::vector<int> &lc = wloc[w];
+      for (int t = 0; t < N.k; ++t) lc[N.p0 + t] = t;
+      for (size_t t = 0; t < N.R.size(); ++t) lc[N.R[t]] = N.roff + (int)t;
+      int *src = P.asm_src[N.depth].data() + off[s];
+      long long *dst = P.asm_dst[N.depth].data() + off[s];
+      long long q = 0;
+      for (int t = 0; t < N.k; ++t) {
+        const int i = P.perm[N.p0 + t];
+        const long long li = t;
+        for (long long p = I[i]; p < I[i + 1]; ++p) {
+          const int vj = P.iperm[J[p]];
+          if (vj < N.p0) continue;
+          const long long lj = lc[vj];
+          if (lj < 0) { outside = 1; continue; }
+          src[q] = (int)p;
+          dst[q++] = N.arena_off + li + lj * N.ld;
+          if (vj >= N.p0 + N.k) {
+            src[q] = P.tpos[p];
+            dst[q++] = N.arena_off + lj + li * N.ld;
+          }
+        }
+      }
+      for (int t = 0; t < N.k; ++t) lc[N.p0 + t] = -1;
+      for (int v : N.R) lc[v] = -1;
+    });
+    if (outside) return fail(LFSOLVE_ERR_ARG, "internal: coupling outside the front");
   }
+  phase("assembly map");
   return LFSOLVE_OK;
 }
 
@@ -1253,6 +1354,14 @@ struct lfsolve {
 
 namespace {
 
+template <typename T>
+int upload(T **dst, const HostBuf<T> &v, cudaStream_t st) {
+  *dst = nullptr;
+  if (v.empty()) return LFSOLVE_OK;
+  LS_CUDA(cudaMalloc((void **)dst, v.size() * sizeof(T)));
+  LS_CUDA(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return LFSOLVE_OK;
+}
 template <typename T>
 int upload(T **dst, const std::vector<T> &v, cudaStream_t st) {
   *dst = nullptr;
